@@ -1,0 +1,457 @@
+#!/usr/bin/env python3
+"""Benchmark of the Ozaki Scheme II FP64 GEMM on B200 (one JSON line on rank 0).
+
+Workload (default): Scheme II, M = N = K = 8192, 16 moduli, inputs
+(U - 0.5) * exp(0.5 * N(0,1)) from the seeded generator (A seed 42, B seed 43),
+row-major FP64.  A "step" is one full GEMM (steps 1-4).  Metric: emulated FP64
+TFLOPS = 2 M N K / step time.  The 1 GiB of inputs exceed the 126 MB L2, so no
+extra L2 flush is done between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--size 8192] [--slices 16] [--scheme 2] [--phi 0.5]
+
+--impl reference times the reference's own CPU implementation of the path
+(its step 1/2/4 kernel source compiled for the host, oracle/_ref, with an
+exact CPU INT8 GEMM for step 3) on a bounded block sample of the same
+workload, on all host cores.
+
+With --gpus N > 1 (torchrun), every rank runs an independent replica of the
+workload on its own GPU (the GEMM has no exchange step): value = N replicas'
+flops / max-over-ranks time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from fractions import Fraction
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "emulated_fp64_tflops"
+UNIT = "TFLOP/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=8192)
+    p.add_argument("--slices", type=int, default=16)
+    p.add_argument("--scheme", type=int, default=2, choices=[1, 2])
+    p.add_argument("--phi", type=float, default=0.5)
+    p.add_argument("--cpu-sample", type=int, default=512, help="rows/cols of the CPU block sample")
+    p.add_argument("--no-extras", action="store_true", help="skip DGEMM / reference-GPU / accuracy side numbers")
+    return p.parse_args()
+
+
+def workload(args):
+    return {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{args.size}^3",
+            "M": args.size, "N": args.size, "K": args.size, "scheme": args.scheme,
+            "slices": args.slices, "phi": args.phi, "input_seeds": [42, 43],
+            "layout": "row-major fp64", "l2": "inputs (1 GiB) larger than L2; no flush"}
+
+
+def int8_ops(args):
+    S = args.slices
+    G = S if args.scheme == 2 else S * (S + 1) // 2
+    return 2.0 * args.size ** 3 * G
+
+
+# ------------------------------------------------------------------ distributed
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ exact sampled reference
+def exact_dot(a_row, b_col):
+    """Correctly rounded double of sum a_k b_k, by exact integer arithmetic."""
+    acc = Fraction(0)
+    terms = []
+    emin = None
+    for x, y in zip(a_row, b_col):
+        if x == 0.0 or y == 0.0:
+            continue
+        mx, ex = math.frexp(x)
+        my, ey = math.frexp(y)
+        ix, iy = int(mx * (1 << 53)), int(my * (1 << 53))
+        e = ex + ey - 106
+        terms.append((ix * iy, e))
+        emin = e if emin is None or e < emin else emin
+    if not terms:
+        return 0.0
+    total = 0
+    for v, e in terms:
+        total += v << (e - emin)
+    acc = Fraction(total) * (Fraction(2) ** emin if emin >= 0 else Fraction(1, 2 ** (-emin)))
+    return float(acc)
+
+
+def sampled_errors(A, B, C_list, nsamp=48, seed=7):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    M, K = A.shape
+    N = B.shape[1]
+    ii = rng.integers(0, M, nsamp)
+    jj = rng.integers(0, N, nsamp)
+    ex = np.array([exact_dot(A[i], B[:, j]) for i, j in zip(ii, jj)])
+    out = []
+    for C in C_list:
+        got = np.array([C[i, j] for i, j in zip(ii, jj)])
+        d = np.abs(got - ex)
+        rel = np.where(ex != 0, d / np.where(ex != 0, np.abs(ex), 1), d)
+        out.append(float(rel.max()))
+    return out
+
+
+# ------------------------------------------------------------------ reference arm (CPU)
+def cpu_reference_sample(args, A, B, steps=1, warmup=0):
+    """The reference's CPU implementation on an ms x ns block of C with full K
+    (each block of the full product is computed exactly as in the full run:
+    row/column shifts depend on full rows of A / columns of B only)."""
+    import numpy as np
+    from oracle import Ref
+    ms = min(args.cpu_sample, A.shape[0])
+    ns = min(args.cpu_sample, B.shape[1])
+    As = np.ascontiguousarray(A[:ms])
+    Bs = np.ascontiguousarray(B[:, :ns])
+    scratch = None
+    for _ in range(warmup):
+        _, scratch = Ref.cpu_pipeline(args.scheme, As, Bs, args.slices, scratch)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        _, scratch = Ref.cpu_pipeline(args.scheme, As, Bs, args.slices, scratch)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    flops = 2.0 * ms * ns * A.shape[1]
+    from oracle import Oracle
+    return {"value": flops / t / 1e12, "unit": UNIT, "cores": Oracle.num_threads(),
+            "kind": "reference", "seconds_per_sample": t,
+            "sample": f"C[0:{ms},0:{ns}] block (full K={A.shape[1]}) of the same GEMM, "
+                      f"scheme {args.scheme}, S={args.slices}: reference step 1/2/4 kernel source on the host "
+                      f"(OpenMP over rows) + exact CPU INT8 GEMM"}
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    import numpy as np
+    import ozablas_b200 as oz
+    n = args.size
+    A = oz.generate_matrix(min(args.cpu_sample, n), n, args.phi, 42)
+    Bfull_cols = min(args.cpu_sample, n)
+    B = oz.generate_matrix(n, n, args.phi, 43)[:, :Bfull_cols] if n <= 8192 else None
+    res = cpu_reference_sample(args, A, np.ascontiguousarray(B), steps=args.steps, warmup=min(args.warmup, 1))
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["seconds_per_sample"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 emulated via int8/int32", "data": "synthetic",
+            "impl": "reference", "config": workload(args),
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def load_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def time_events(fn, steps, stream):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record(stream)
+    for _ in range(steps):
+        fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / steps
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+    import ozablas_b200 as oz
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, S = args.size, args.slices
+    hA = oz.generate_matrix(n, n, args.phi, 42)
+    hB = oz.generate_matrix(n, n, args.phi, 43)
+    pA = torch.from_numpy(hA).pin_memory()
+    pB = torch.from_numpy(hB).pin_memory()
+    dA = pA.to(dev)
+    dB = pB.to(dev)
+    dC = torch.empty(n, n, dtype=torch.float64, device=dev)
+    ex = oz.CudaExecutor(local)
+    stream = torch.cuda.current_stream(dev)
+    ex.set_stream(stream.cuda_stream)
+    W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, n, n, n, S)
+    gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
+    step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        ms = time_events(step, args.steps, stream)
+    barrier(ws)
+    ms = dist_max(ms, ws)
+    flops = 2.0 * n ** 3
+    value = ws * flops / (ms * 1e-3) / 1e12
+
+    # per-step breakdown and the GEMM kernel's own duration (events around the launch)
+    t = oz.OzaTimings()
+    acc = [0.0] * 5
+    reps = max(3, min(args.steps, 10))
+    for _ in range(reps):
+        gemm(W, dA, dB, dC, t)
+        for i, f in enumerate(("step1_ms", "step2_ms", "step3_ms", "step4_ms", "total_ms")):
+            acc[i] += getattr(t, f) / reps
+    step_ms = dict(zip(("step1_ms", "step2_ms", "step3_ms", "step4_ms", "total_ms"), acc))
+
+    # end to end through the public API: host buffers, copies inside the timed region
+    hC = torch.empty(n, n, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        dA.copy_(pA, non_blocking=True)
+        dB.copy_(pB, non_blocking=True)
+        gemm(W, dA, dB, dC)
+        hC.copy_(dC, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier(ws)
+    e2e_ms = dist_max(time_events(e2e_step, args.steps, stream), ws)
+
+    peaks, peak_src = load_peaks()
+    extras = {}
+    int8_peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
+    int8_peak_src = f"2 x bf16 {peak_src} burst ({peaks.get('bf16_tflops')} TF): dense int8 rate of sm_100 is twice bf16"
+    if rank == 0 and not args.no_extras:
+        # cuBLAS INT8 GEMM (torch._int_mm) at the same size, for the INT8 peak reference
+        try:
+            a8 = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
+            b8 = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
+            for _ in range(3):
+                torch._int_mm(a8, b8)
+            i8ms = time_events(lambda: torch._int_mm(a8, b8), 10, stream)
+            extras["cublas_int8_tops"] = 2.0 * n ** 3 / (i8ms * 1e-3) / 1e12
+            del a8, b8
+        except Exception as e:  # noqa: BLE001
+            extras["cublas_int8_tops"] = f"unavailable: {e}"
+        if isinstance(extras.get("cublas_int8_tops"), float) and extras["cublas_int8_tops"] > int8_peak:
+            int8_peak = extras["cublas_int8_tops"]
+            int8_peak_src = "measured cuBLAS int8 GEMM at the same size (torch._int_mm)"
+        # native cuBLAS DGEMM
+        dD = torch.empty_like(dC)
+        for _ in range(2):
+            torch.matmul(dA, dB, out=dD)
+        dms = time_events(lambda: torch.matmul(dA, dB, out=dD), max(3, args.steps // 2), stream)
+        extras["cublas_dgemm_tflops"] = flops / (dms * 1e-3) / 1e12
+        # reference GPU pipeline (cuBLAS-backed), if built
+        extras["reference_gpu_pipeline_tflops"] = reference_gpu_tflops(args, dA, dB, stream)
+        # accuracy against an exact sampled reference, beside DGEMM's
+        C_ours = dC.cpu().numpy()
+        C_dgemm = dD.cpu().numpy()
+        e_ours, e_dgemm = sampled_errors(hA, hB, [C_ours, C_dgemm])
+        extras["max_rel_err_sampled"] = {"ours": e_ours, "cublas_dgemm": e_dgemm, "samples": 48,
+                                         "reference": "exact (rational) dot products, rounded once"}
+        del dD
+
+    gemm_ms = step_ms["step3_ms"]
+    achieved = int8_ops(args) / (gemm_ms * 1e-3) / 1e12
+    traffic = load_traffic().get(f"gemm_i8_{n}_S{S}_scheme{args.scheme}")
+    bytes_h2d = 2 * n * n * 8
+    bytes_d2h = n * n * 8
+    steps_kernels = 6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 emulated via int8 x int8 -> int32 (tcgen05 kind::i8)", "data": "synthetic",
+        "impl": "ours", "config": workload(args),
+        "parallelism": "replicas" if ws > 1 else "single",
+        "e2e": {"value": ws * flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT, "h2d_bytes_per_step": bytes_h2d,
+                "d2h_bytes_per_step": bytes_d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": steps_kernels * args.steps,
+        "steps_ms": step_ms,
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_i8", "achieved": achieved, "peak": int8_peak,
+                     "unit": "TOPS (int8)", "frac": achieved / int8_peak, "peak_source": int8_peak_src,
+                     "traffic": traffic,
+                     "algorithmic": f"2*M*N*K*{'S' if args.scheme == 2 else 'S(S+1)/2'} int8 ops per launch"},
+        "clocks": clk.summary(),
+    }
+    line.update(extras)
+    if rank == 0:
+        try:
+            line["cpu_baseline"] = cpu_baseline_leg(args, hA, hB)
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_leg(args, hA, hB):
+    import numpy as np
+    ms = min(args.cpu_sample, hA.shape[0])
+    ns = min(args.cpu_sample, hB.shape[1])
+    res = cpu_reference_sample(args, np.ascontiguousarray(hA[:ms]), np.ascontiguousarray(hB[:, :ns]), steps=1)
+    return {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+
+def reference_gpu_tflops(args, dA, dB, stream):
+    import ctypes
+    import torch
+    so = os.path.join(ROOT, "baseline", "_ref", "libozablas_ref_gpu.so")
+    if not os.path.exists(so):
+        return "unavailable: baseline/_ref not built"
+    n = args.size
+    if args.scheme == 2 and args.slices * n * n >= 2 ** 31:
+        return "unavailable: the reference's 32-bit index arithmetic overflows at this size"
+    L = ctypes.CDLL(so)
+    L.refgpu_init.argtypes = [ctypes.c_int]
+    L.refgpu_ws_create.restype = ctypes.c_void_p
+    L.refgpu_ws_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int]
+    L.refgpu_gemm.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.refgpu_ws_destroy.argtypes = [ctypes.c_void_p]
+    if L.refgpu_init(torch.cuda.current_device()) != 0:
+        return "unavailable: executor init failed"
+    h = L.refgpu_ws_create(args.scheme, n, n, n, args.slices)
+    if not h:
+        return "unavailable: workspace allocation failed"
+    dR = torch.empty(n, n, dtype=torch.float64, device=dA.device)
+    # the reference issues on the legacy default stream
+    torch.cuda.synchronize()
+    run = lambda: L.refgpu_gemm(h, dA.data_ptr(), dB.data_ptr(), dR.data_ptr(), None)  # noqa: E731
+    for _ in range(2):
+        run()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        run()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    L.refgpu_ws_destroy(h)
+    return 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

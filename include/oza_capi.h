@@ -1,0 +1,146 @@
+/*
+ * oza_capi.h -- C ABI of the B200-native Ozaki Scheme I / II FP64 GEMM.
+ *
+ * Plain C: opaque handles, device pointers and sizes; no CUDA or C++ types in
+ * any signature.  The C++ drop-in API (<ozablas/ozablas.hpp>,
+ * <ozablas/core/executor.hpp>, <ozablas/core/workspace.hpp>) is implemented on
+ * top of these entry points, and the Python bindings (ozablas_b200) load them
+ * with ctypes.  Each entry point names the reference interface it replaces
+ * (paths relative to the IlyaNyrkov/ozablas source tree).
+ *
+ * Conventions (same as the reference, include/ozablas/ozablas.hpp:13-31):
+ *   A is M x K, B is K x N, C is M x N, all row-major FP64 device buffers with
+ *   leading dimensions K, N, N.  C is fully overwritten.  No alpha, beta or
+ *   transposes.  Work is issued on the executor's stream (default: the legacy
+ *   default stream, as in the reference); the call returns asynchronously
+ *   unless a timings struct is passed, in which case it waits for the result.
+ *   Inputs must be finite.
+ */
+#ifndef OZA_CAPI_H
+#define OZA_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum oza_status {
+    OZA_OK = 0,
+    OZA_INVALID_ARG = 1,   /* -> std::invalid_argument in the C++ layer      */
+    OZA_OOM = 2,           /* -> std::bad_alloc                                */
+    OZA_CUDA_ERROR = 3,    /* -> std::runtime_error                            */
+    OZA_TIMEOUT = 4,       /* a bounded device-side wait expired               */
+    OZA_UNSUPPORTED = 5    /* valid request this build cannot serve            */
+} oza_status_t;
+
+typedef struct oza_executor* oza_exec_t;
+typedef struct oza_workspace* oza_ws_t;
+
+/* Per-step device times in milliseconds.
+ * Reference: struct OzaTimings, include/ozablas/core/workspace.hpp:97-103. */
+typedef struct oza_timings {
+    float step1_ms;  /* exponent statistics                         */
+    float step2_ms;  /* slicing / residues                          */
+    float step3_ms;  /* INT8 tensor-core products                   */
+    float step4_ms;  /* scaled sum / CRT reconstruction             */
+    float total_ms;
+} oza_timings_t;
+
+/* Schemes. */
+#define OZA_SCHEME1 1  /* sum-and-scale slices */
+#define OZA_SCHEME2 2  /* CRT residues          */
+
+/* Workspace flags. */
+#define OZA_WS_MATERIALIZE 0x1u  /* keep every intermediate (slices, INT32 products) in
+                                    the workspace buffers, for inspection and parity */
+
+/* Buffers exposed by oza_ws_get_ptr (reference getters workspace.hpp:174-178). */
+#define OZA_BUF_SHIFT_A  0  /* int32[M]                                      */
+#define OZA_BUF_SHIFT_B  1  /* int32[N]                                      */
+#define OZA_BUF_A_SLICES 2  /* int8 [S][Mp][Kp]   (K-major, zero padded)     */
+#define OZA_BUF_B_SLICES 3  /* int8 [S][Np][Kp]   (K-major: B transposed)    */
+#define OZA_BUF_C_TC     4  /* int32[G][Mp][Np]   (only with MATERIALIZE)    */
+
+/* Workspace geometry (padded extents of the buffers above). */
+typedef struct oza_ws_info {
+    int scheme, slices;
+    size_t M, N, K;
+    size_t Mp, Np, Kp;     /* padded extents used by the device layouts   */
+    int groups;            /* INT32 product planes: S (II) or S (I, one per group g=2..S+1) */
+    int k_param;           /* Scheme II: K_param of step 1; Scheme I: 0   */
+    int beta;              /* Scheme I: slice width beta; Scheme II: 0    */
+    unsigned flags;
+    size_t bytes;          /* device bytes held by the workspace          */
+} oza_ws_info_t;
+
+/* ---- errors -------------------------------------------------------------- */
+/* Thread-local text of the last failure of any entry point on this thread. */
+const char* oza_last_error_string(void);
+
+/* ---- executor ------------------------------------------------------------ */
+/* Reference: CudaExecutor::CudaExecutor(int), src/core/executor.cpp:61-70. */
+oza_status_t oza_executor_create(int device, oza_exec_t* out);
+/* Reference: CudaExecutor::~CudaExecutor, executor.cpp:72-76. */
+oza_status_t oza_executor_destroy(oza_exec_t ex);
+/* Reference: Executor::allocate / free, executor.hpp:19-24 (executor.cpp:78-86). */
+oza_status_t oza_executor_alloc(oza_exec_t ex, void** ptr, size_t bytes);
+oza_status_t oza_executor_free(oza_exec_t ex, void* ptr);
+/* kind: 1 host->device, 2 device->host, 3 device->device.
+ * Reference: copy_from_host / copy_to_host / copy_device_to_device, executor.cpp:88-104. */
+oza_status_t oza_executor_copy(oza_exec_t ex, void* dst, const void* src, size_t bytes, int kind);
+/* Reference: Executor::synchronize, executor.cpp:106-110. */
+oza_status_t oza_executor_synchronize(oza_exec_t ex);
+/* Extension (no reference counterpart): issue work on a caller cudaStream_t
+ * (passed as void*; NULL = legacy default stream). */
+oza_status_t oza_executor_set_stream(oza_exec_t ex, void* stream);
+oza_status_t oza_executor_device(oza_exec_t ex, int* device);
+/* Reference: Executor::get_blas_handle, executor.hpp:35 -- a cuBLAS handle
+ * created on first use (the GEMM path itself never calls cuBLAS); NULL if
+ * libcublas cannot be loaded. */
+void* oza_executor_blas_handle(oza_exec_t ex);
+
+/* ---- workspace ----------------------------------------------------------- */
+/* Reference: WorkspaceScheme1/2 constructors, src/core/workspace.cpp:21-47, 65-114.
+ * Scheme I requires slices >= 1, Scheme II 1 <= slices <= 20. */
+oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, int slices,
+                           unsigned flags, oza_ws_t* out);
+/* Reference: ~WorkspaceScheme1/2, workspace.cpp:49-56, 117-124. */
+oza_status_t oza_ws_destroy(oza_ws_t ws);
+/* Reference: get_shift_A/B, get_A_slices/get_B_slices, get_C_tc (workspace.hpp:174-178). */
+oza_status_t oza_ws_get_ptr(oza_ws_t ws, int which, void** ptr);
+oza_status_t oza_ws_get_info(oza_ws_t ws, oza_ws_info_t* info);
+
+/* ---- the GEMM ------------------------------------------------------------ */
+/* C = A * B by the workspace's scheme.
+ * Reference: ozablas::ozaki_scheme1_gemm / ozaki_scheme2_gemm
+ * (include/ozablas/ozablas.hpp:20,31; src/ozablas.cpp:22-74; src/cuda/pipeline.cu:40-265).
+ * timings may be NULL (asynchronous call). */
+oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, oza_timings_t* timings);
+
+/* Device error word of the last launch sequence on this workspace: 0 = none,
+ * otherwise a bounded wait expired inside a kernel (the call then returned
+ * OZA_TIMEOUT). */
+oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
+
+/* ---- host utilities ------------------------------------------------------- */
+/* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from
+ * std::mt19937(seed) in row-major order.
+ * Reference: matrix_utils::generation::generate_ozaki_matrix, utils/matrix_gen.hpp:15-34. */
+oza_status_t oza_generate_matrix(int rows, int cols, double phi, int seed, double* out);
+
+/* Scheme parameters computed on the host.
+ * Reference: calculate_scheme1_beta / calculate_scheme2_k_param,
+ * src/pipeline/step1_statistics.hpp:12-20 (K_param with M as in pipeline.cu:196-198). */
+int oza_scheme1_beta(size_t K);
+int oza_scheme2_k_param(int slices, size_t K);
+
+/* Library version string. */
+const char* oza_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OZA_CAPI_H */

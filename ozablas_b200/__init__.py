@@ -1,0 +1,319 @@
+"""ozablas_b200 -- B200-native Ozaki Scheme I / II FP64 GEMM.
+
+Python mirror of the OzaBLAS operator interface (IlyaNyrkov/ozablas:
+include/ozablas/ozablas.hpp:20,31, core/executor.hpp, core/workspace.hpp)
+over the C ABI of include/oza_capi.h, loaded from the in-tree
+``liboza_b200.so``.  The arithmetic runs only in the sm_100a kernels of that
+library; there is no CPU fallback, and every entry point raises if the
+library or a B200 is missing.
+
+Matrices are row-major FP64 device buffers, passed either as raw device
+pointers (int) or as contiguous CUDA ``torch.float64`` tensors.
+
+    ex = CudaExecutor(0)
+    ws = WorkspaceScheme2(ex, M, N, K, slices=16)
+    ozaki_scheme2_gemm(ws, A, B, C)            # asynchronous
+    t = OzaTimings(); ozaki_scheme2_gemm(ws, A, B, C, t)   # synchronous, per-step ms
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from dataclasses import dataclass
+
+__all__ = [
+    "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
+    "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
+    "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboza_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "oza_capi.h")
+
+OZA_OK, OZA_INVALID_ARG, OZA_OOM, OZA_CUDA_ERROR, OZA_TIMEOUT, OZA_UNSUPPORTED = range(6)
+OZA_SCHEME1, OZA_SCHEME2 = 1, 2
+OZA_WS_MATERIALIZE = 0x1
+BUF_SHIFT_A, BUF_SHIFT_B, BUF_A_SLICES, BUF_B_SLICES, BUF_C_TC = range(5)
+
+
+class OzaError(RuntimeError):
+    """CUDA failure or unsupported request (std::runtime_error in the C++ API)."""
+
+
+class OzaTimeoutError(OzaError):
+    """A bounded device-side wait expired inside a kernel."""
+
+
+class _Timings(ctypes.Structure):
+    _fields_ = [("step1_ms", ctypes.c_float), ("step2_ms", ctypes.c_float), ("step3_ms", ctypes.c_float),
+                ("step4_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+
+
+class _WsInfo(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("slices", ctypes.c_int),
+                ("M", ctypes.c_size_t), ("N", ctypes.c_size_t), ("K", ctypes.c_size_t),
+                ("Mp", ctypes.c_size_t), ("Np", ctypes.c_size_t), ("Kp", ctypes.c_size_t),
+                ("groups", ctypes.c_int), ("k_param", ctypes.c_int), ("beta", ctypes.c_int),
+                ("flags", ctypes.c_uint), ("bytes", ctypes.c_size_t)]
+
+
+@dataclass
+class OzaTimings:
+    """Per-step device milliseconds (reference: struct OzaTimings, workspace.hpp:97-103)."""
+    step1_ms: float = 0.0
+    step2_ms: float = 0.0
+    step3_ms: float = 0.0
+    step4_ms: float = 0.0
+    total_ms: float = 0.0
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C-ABI library; raises OSError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: build it with `make -C ozablas_b200/csrc` "
+                      "(or __graft_entry__.build()); there is no fallback implementation")
+    L = ctypes.CDLL(LIB_PATH)
+    P, S, I, U = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint
+    sig = {
+        "oza_last_error_string": (ctypes.c_char_p, []),
+        "oza_version": (ctypes.c_char_p, []),
+        "oza_executor_create": (I, [I, ctypes.POINTER(P)]),
+        "oza_executor_destroy": (I, [P]),
+        "oza_executor_alloc": (I, [P, ctypes.POINTER(P), S]),
+        "oza_executor_free": (I, [P, P]),
+        "oza_executor_copy": (I, [P, P, P, S, I]),
+        "oza_executor_synchronize": (I, [P]),
+        "oza_executor_set_stream": (I, [P, P]),
+        "oza_executor_device": (I, [P, ctypes.POINTER(I)]),
+        "oza_executor_blas_handle": (P, [P]),
+        "oza_ws_create": (I, [P, I, S, S, S, I, U, ctypes.POINTER(P)]),
+        "oza_ws_destroy": (I, [P]),
+        "oza_ws_get_ptr": (I, [P, I, ctypes.POINTER(P)]),
+        "oza_ws_get_info": (I, [P, ctypes.POINTER(_WsInfo)]),
+        "oza_gemm": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
+        "oza_ws_device_error": (I, [P, ctypes.POINTER(I)]),
+        "oza_generate_matrix": (I, [I, I, ctypes.c_double, I, P]),
+        "oza_scheme1_beta": (I, [S]),
+        "oza_scheme2_k_param": (I, [I, S]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype, fn.argtypes = res, args
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Every function name declared in include/oza_capi.h."""
+    with open(HEADER_PATH) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(oza_[a-z0-9_]+)\s*\(", text)))
+
+
+def _check(status: int) -> None:
+    if status == OZA_OK:
+        return
+    msg = (lib().oza_last_error_string() or b"").decode(errors="replace")
+    if status == OZA_INVALID_ARG:
+        raise ValueError(msg)
+    if status == OZA_OOM:
+        raise MemoryError(msg)
+    if status == OZA_TIMEOUT:
+        raise OzaTimeoutError(msg)
+    raise OzaError(msg)
+
+
+def _ptr(x) -> int:
+    """Device address of an int or of a contiguous CUDA float64 torch tensor."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda:
+            raise ValueError("matrix must live on the GPU (no CPU fallback)")
+        if not x.is_contiguous():
+            raise ValueError("matrix must be contiguous (row-major)")
+        return int(x.data_ptr())
+    raise TypeError(f"expected a device pointer or a CUDA tensor, got {type(x).__name__}")
+
+
+class CpuExecutor:
+    """Host executor kept for API compatibility; the GEMMs reject it, as the
+    reference's dispatcher does (src/ozablas.cpp:42-45)."""
+
+
+class CudaExecutor:
+    """Device, stream and allocations (reference CudaExecutor, executor.cpp:61-114)."""
+
+    def __init__(self, device_id: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().oza_executor_create(int(device_id), ctypes.byref(h)))
+        self._h = h
+        self.device_id = int(device_id)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def allocate(self, nbytes: int) -> int:
+        p = ctypes.c_void_p()
+        _check(lib().oza_executor_alloc(self._h, ctypes.byref(p), int(nbytes)))
+        return int(p.value or 0)
+
+    def free(self, ptr: int) -> None:
+        _check(lib().oza_executor_free(self._h, ctypes.c_void_p(ptr)))
+
+    def copy_from_host(self, dst: int, src: int, nbytes: int) -> None:
+        _check(lib().oza_executor_copy(self._h, ctypes.c_void_p(dst), ctypes.c_void_p(src), int(nbytes), 1))
+
+    def copy_to_host(self, dst: int, src: int, nbytes: int) -> None:
+        _check(lib().oza_executor_copy(self._h, ctypes.c_void_p(dst), ctypes.c_void_p(src), int(nbytes), 2))
+
+    def copy_device_to_device(self, dst: int, src: int, nbytes: int) -> None:
+        _check(lib().oza_executor_copy(self._h, ctypes.c_void_p(dst), ctypes.c_void_p(src), int(nbytes), 3))
+
+    def synchronize(self) -> None:
+        _check(lib().oza_executor_synchronize(self._h))
+
+    def set_stream(self, stream) -> None:
+        """Issue subsequent work on a CUDA stream (int handle, torch.cuda.Stream, or None)."""
+        s = getattr(stream, "cuda_stream", stream)
+        _check(lib().oza_executor_set_stream(self._h, ctypes.c_void_p(int(s or 0))))
+
+    def get_blas_handle(self) -> int:
+        return int(lib().oza_executor_blas_handle(self._h) or 0)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.oza_executor_destroy(h)
+            self._h = None
+
+
+class _Workspace:
+    _scheme = 0
+
+    def __init__(self, executor, M: int, N: int, K: int, slices: int, materialize: bool = False):
+        if executor is None:
+            raise ValueError("OzaBLAS: Executor cannot be null.")
+        if not isinstance(executor, CudaExecutor):
+            raise OzaError("OzaBLAS: No suitable hardware backend found for the provided Executor.")
+        self._exec = executor   # keeps the executor alive, like the reference's shared_ptr
+        h = ctypes.c_void_p()
+        flags = OZA_WS_MATERIALIZE if materialize else 0
+        _check(lib().oza_ws_create(executor.handle, self._scheme, int(M), int(N), int(K), int(slices),
+                                   flags, ctypes.byref(h)))
+        self._h = h
+        info = _WsInfo()
+        _check(lib().oza_ws_get_info(h, ctypes.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in _WsInfo._fields_}
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_executor(self):
+        return self._exec
+
+    def get_M(self): return self.info["M"]
+    def get_N(self): return self.info["N"]
+    def get_K(self): return self.info["K"]
+    def get_slices(self): return self.info["slices"]
+    def get_Mp(self): return self.info["Mp"]
+    def get_Np(self): return self.info["Np"]
+    def get_Kp(self): return self.info["Kp"]
+
+    def _buf(self, which: int) -> int:
+        p = ctypes.c_void_p()
+        _check(lib().oza_ws_get_ptr(self._h, which, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def get_shift_A(self): return self._buf(BUF_SHIFT_A)
+    def get_shift_B(self): return self._buf(BUF_SHIFT_B)
+    def get_A_slices(self): return self._buf(BUF_A_SLICES)
+    def get_B_slices(self): return self._buf(BUF_B_SLICES)
+    def get_C_tc(self): return self._buf(BUF_C_TC)
+
+    def device_error(self) -> int:
+        c = ctypes.c_int()
+        _check(lib().oza_ws_device_error(self._h, ctypes.byref(c)))
+        return c.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.oza_ws_destroy(h)
+            self._h = None
+
+
+class WorkspaceScheme1(_Workspace):
+    """Scheme I workspace (reference WorkspaceScheme1, workspace.cpp:21-56); slices >= 1."""
+    _scheme = OZA_SCHEME1
+
+
+class WorkspaceScheme2(_Workspace):
+    """Scheme II workspace (reference WorkspaceScheme2, workspace.cpp:63-126); 1 <= slices <= 20."""
+    _scheme = OZA_SCHEME2
+
+
+def _gemm(ws, A, B, C, timings):
+    t = _Timings() if timings is not None else None
+    _check(lib().oza_gemm(ws.handle, ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)),
+                          ctypes.c_void_p(_ptr(C)), ctypes.byref(t) if t is not None else None))
+    if timings is not None:
+        for f, _ in _Timings._fields_:
+            setattr(timings, f, float(getattr(t, f)))
+
+
+def _check_shapes(ws, A, B, C):
+    if hasattr(A, "shape") and hasattr(B, "shape") and hasattr(C, "shape"):
+        M, N, K = ws.get_M(), ws.get_N(), ws.get_K()
+        if tuple(A.shape) != (M, K) or tuple(B.shape) != (K, N) or tuple(C.shape) != (M, N):
+            raise ValueError(f"shapes {tuple(A.shape)} x {tuple(B.shape)} -> {tuple(C.shape)} "
+                             f"do not match the workspace ({M}x{K} x {K}x{N})")
+        for t in (A, B, C):
+            if str(getattr(t, "dtype", "torch.float64")) != "torch.float64":
+                raise ValueError("matrices must be float64")
+
+
+def ozaki_scheme1_gemm(ws: WorkspaceScheme1, A, B, C, timings: OzaTimings | None = None) -> None:
+    """C = A * B by Ozaki Scheme I (reference ozaki_scheme1_gemm, ozablas.hpp:20)."""
+    if not isinstance(ws, WorkspaceScheme1):
+        raise TypeError("ozaki_scheme1_gemm needs a WorkspaceScheme1")
+    _check_shapes(ws, A, B, C)
+    _gemm(ws, A, B, C, timings)
+
+
+def ozaki_scheme2_gemm(ws: WorkspaceScheme2, A, B, C, timings: OzaTimings | None = None) -> None:
+    """C = A * B by Ozaki Scheme II (reference ozaki_scheme2_gemm, ozablas.hpp:31)."""
+    if not isinstance(ws, WorkspaceScheme2):
+        raise TypeError("ozaki_scheme2_gemm needs a WorkspaceScheme2")
+    _check_shapes(ws, A, B, C)
+    _gemm(ws, A, B, C, timings)
+
+
+def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):
+    """Seeded (U-0.5)*exp(phi*N(0,1)) matrix as a numpy array (reference
+    generate_ozaki_matrix, utils/matrix_gen.hpp:15-34)."""
+    import numpy as np
+    out = np.empty((rows, cols), dtype=np.float64)
+    _check(lib().oza_generate_matrix(int(rows), int(cols), float(phi), int(seed),
+                                     out.ctypes.data_as(ctypes.c_void_p)))
+    return out
+
+
+def scheme1_beta(K: int) -> int:
+    return int(lib().oza_scheme1_beta(int(K)))
+
+
+def scheme2_k_param(slices: int, K: int) -> int:
+    return int(lib().oza_scheme2_k_param(int(slices), int(K)))

@@ -1,0 +1,465 @@
+// oza_capi.cpp -- host side of the C ABI declared in include/oza_capi.h:
+// executor (device, stream, allocations), workspaces (padded device layouts)
+// and the stage orchestration of Scheme I / Scheme II.
+//
+// Orchestration follows the reference's four steps (src/cuda/pipeline.cu:40-265)
+// with its observable contract: per-step OzaTimings measured with CUDA events,
+// asynchronous unless timings are requested, C fully overwritten.
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <random>
+#include <string>
+
+#include "oza_capi.h"
+#include "oza_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+oza_status_t fail(oza_status_t st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+oza_status_t cuda_fail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(OZA_OOM, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return fail(OZA_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define OZA_CUDA_TRY(call, what)                   \
+    do {                                           \
+        cudaError_t e__ = (call);                  \
+        if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+    } while (0)
+
+}  // namespace
+
+struct oza_executor {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;   // legacy default stream unless set
+    void* blas = nullptr;            // cuBLAS handle created on first request
+    std::mutex blas_mu;
+};
+
+struct oza_workspace {
+    oza_executor* ex = nullptr;
+    int scheme = 0, S = 0;
+    size_t M = 0, N = 0, K = 0, Mp = 0, Np = 0, Kp = 0;
+    int groups = 0, k_param = 0, beta = 0;
+    unsigned flags = 0;
+    size_t bytes = 0;
+    int32_t* shiftA = nullptr;
+    int32_t* shiftB = nullptr;
+    unsigned long long* colmax = nullptr;
+    int8_t* aplanes = nullptr;
+    int8_t* bplanes = nullptr;
+    int32_t* ctc = nullptr;
+    int* err = nullptr;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    oza::PairList pairs{};
+};
+
+namespace {
+
+// Make the executor's device current for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void ws_release(oza_workspace* ws) {
+    void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->err};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    for (auto& e : ws->ev)
+        if (e) cudaEventDestroy(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oza_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* oza_version(void) { return "ozablas_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------- executor
+oza_status_t oza_executor_create(int device, oza_exec_t* out) {
+    if (!out) return fail(OZA_INVALID_ARG, "oza_executor_create: null output handle");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return cuda_fail(e, "CUDA: no usable device");
+    if (device < 0 || device >= count) return fail(OZA_INVALID_ARG, "CUDA: device %d out of range (%d)", device, count);
+    OZA_CUDA_TRY(cudaSetDevice(device), "CUDA: Failed to set device");
+    int major = 0, minor = 0, sms = 0;
+    OZA_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "CUDA: attribute");
+    OZA_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device), "CUDA: attribute");
+    OZA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "CUDA: attribute");
+    if (major != 10 || minor != 0)
+        return fail(OZA_UNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a (B200) only", device, major,
+                    minor);
+    auto* ex = new (std::nothrow) oza_executor();
+    if (!ex) return fail(OZA_OOM, "oza_executor_create: host allocation failed");
+    ex->device = device;
+    ex->sms = sms;
+    *out = ex;
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_destroy(oza_exec_t ex) {
+    if (!ex) return OZA_OK;
+    if (ex->blas) {
+        void* lib = dlopen("libcublas.so.12", RTLD_NOW | RTLD_NOLOAD);
+        if (lib) {
+            auto destroy = reinterpret_cast<int (*)(void*)>(dlsym(lib, "cublasDestroy_v2"));
+            if (destroy) destroy(ex->blas);
+        }
+    }
+    delete ex;
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_alloc(oza_exec_t ex, void** ptr, size_t bytes) {
+    if (!ex || !ptr) return fail(OZA_INVALID_ARG, "oza_executor_alloc: null argument");
+    DeviceGuard g(ex->device);
+    *ptr = nullptr;
+    cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(OZA_OOM, "CUDA: allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
+    }
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_free(oza_exec_t ex, void* ptr) {
+    if (!ex) return fail(OZA_INVALID_ARG, "oza_executor_free: null executor");
+    if (!ptr) return OZA_OK;
+    DeviceGuard g(ex->device);
+    OZA_CUDA_TRY(cudaFree(ptr), "CUDA: free failed");
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_copy(oza_exec_t ex, void* dst, const void* src, size_t bytes, int kind) {
+    if (!ex || (!dst && bytes) || (!src && bytes)) return fail(OZA_INVALID_ARG, "oza_executor_copy: null argument");
+    cudaMemcpyKind k;
+    const char* what;
+    switch (kind) {
+        case 1: k = cudaMemcpyHostToDevice; what = "CUDA: Memcpy HostToDevice failed"; break;
+        case 2: k = cudaMemcpyDeviceToHost; what = "CUDA: Memcpy DeviceToHost failed"; break;
+        case 3: k = cudaMemcpyDeviceToDevice; what = "CUDA: Memcpy DeviceToDevice failed"; break;
+        default: return fail(OZA_INVALID_ARG, "oza_executor_copy: kind %d", kind);
+    }
+    if (!bytes) return OZA_OK;
+    DeviceGuard g(ex->device);
+    OZA_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, ex->stream), what);
+    OZA_CUDA_TRY(cudaStreamSynchronize(ex->stream), what);
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_synchronize(oza_exec_t ex) {
+    if (!ex) return fail(OZA_INVALID_ARG, "oza_executor_synchronize: null executor");
+    DeviceGuard g(ex->device);
+    OZA_CUDA_TRY(cudaDeviceSynchronize(), "CUDA: Device synchronize failed");
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_set_stream(oza_exec_t ex, void* stream) {
+    if (!ex) return fail(OZA_INVALID_ARG, "oza_executor_set_stream: null executor");
+    ex->stream = static_cast<cudaStream_t>(stream);
+    return OZA_OK;
+}
+
+oza_status_t oza_executor_device(oza_exec_t ex, int* device) {
+    if (!ex || !device) return fail(OZA_INVALID_ARG, "oza_executor_device: null argument");
+    *device = ex->device;
+    return OZA_OK;
+}
+
+void* oza_executor_blas_handle(oza_exec_t ex) {
+    if (!ex) return nullptr;
+    std::lock_guard<std::mutex> lk(ex->blas_mu);
+    if (ex->blas) return ex->blas;
+    void* lib = dlopen("libcublas.so.12", RTLD_NOW | RTLD_GLOBAL);
+    if (!lib) return nullptr;
+    auto create = reinterpret_cast<int (*)(void**)>(dlsym(lib, "cublasCreate_v2"));
+    if (!create) return nullptr;
+    DeviceGuard g(ex->device);
+    void* h = nullptr;
+    if (create(&h) != 0) return nullptr;
+    ex->blas = h;
+    return h;
+}
+
+// ---------------------------------------------------------------- workspace
+oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, int slices, unsigned flags,
+                           oza_ws_t* out) {
+    if (!out) return fail(OZA_INVALID_ARG, "oza_ws_create: null output handle");
+    *out = nullptr;
+    if (!ex) return fail(OZA_INVALID_ARG, "OzaBLAS: Executor cannot be null.");
+    if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return fail(OZA_INVALID_ARG, "OzaBLAS: unknown scheme %d", scheme);
+    if (scheme == OZA_SCHEME1 && slices < 1) return fail(OZA_INVALID_ARG, "OzaBLAS: Slices must be >= 1.");
+    if (scheme == OZA_SCHEME2 && (slices < 1 || slices > 20))
+        return fail(OZA_INVALID_ARG, "OzaBLAS: Scheme II supports between 1 and 20 slices.");
+    if (scheme == OZA_SCHEME1 && slices > 20)
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: Scheme I is built for at most 20 slices (got %d)", slices);
+    if (flags & ~OZA_WS_MATERIALIZE) return fail(OZA_INVALID_ARG, "oza_ws_create: unknown flags 0x%x", flags);
+
+    auto* ws = new (std::nothrow) oza_workspace();
+    if (!ws) return fail(OZA_OOM, "oza_ws_create: host allocation failed");
+    ws->ex = ex;
+    ws->scheme = scheme;
+    ws->S = slices;
+    ws->M = M;
+    ws->N = N;
+    ws->K = K;
+    ws->Mp = oza::round_up(M, oza::kTileM);
+    ws->Np = oza::round_up(N, oza::kTileN);
+    ws->Kp = oza::round_up(K, oza::kTileK);
+    ws->groups = slices;
+    ws->flags = flags;
+    ws->pairs = oza::make_pairs(scheme, slices);
+    if (scheme == OZA_SCHEME2) ws->k_param = K ? oza_scheme2_k_param(slices, K) : 0;
+    else ws->beta = K ? oza_scheme1_beta(K) : 1;
+
+    // TMA coordinates are 32-bit: plane rows must stay below 2^31.
+    if ((double)slices * (double)ws->Mp >= 2147483648.0 || (double)slices * (double)ws->Np >= 2147483648.0 ||
+        ws->Kp >= (1ull << 31)) {
+        delete ws;
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: problem too large for one workspace (M=%zu N=%zu K=%zu S=%d)", M, N,
+                    K, slices);
+    }
+    // Scheme II products must stay exact in INT32: K * 125^2 < 2^31.
+    if (scheme == OZA_SCHEME2 && (double)K * 125.0 * 125.0 >= 2147483648.0) {
+        delete ws;
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: K=%zu exceeds the INT32-exact bound of Scheme II (K <= 137438)", K);
+    }
+
+    DeviceGuard g(ex->device);
+    cudaError_t e = oza::upload_tables();
+    if (e != cudaSuccess) {
+        delete ws;
+        return cuda_fail(e, "CUDA: constant table upload failed");
+    }
+    struct Req {
+        void** p;
+        size_t bytes;
+    } reqs[] = {
+        {(void**)&ws->shiftA, (M ? M : 1) * sizeof(int32_t)},
+        {(void**)&ws->shiftB, (N ? N : 1) * sizeof(int32_t)},
+        {(void**)&ws->colmax, (N ? N : 1) * sizeof(unsigned long long)},
+        {(void**)&ws->aplanes, (size_t)slices * ws->Mp * ws->Kp + 16},
+        {(void**)&ws->bplanes, (size_t)slices * ws->Np * ws->Kp + 16},
+        {(void**)&ws->ctc, (size_t)ws->groups * ws->Mp * ws->Np * sizeof(int32_t) + 16},
+        {(void**)&ws->err, sizeof(int)},
+    };
+    for (auto& r : reqs) {
+        e = cudaMalloc(r.p, r.bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ws_release(ws);
+            delete ws;
+            return fail(OZA_OOM, "OzaBLAS: workspace allocation of %zu bytes failed", r.bytes);
+        }
+        ws->bytes += r.bytes;
+    }
+    e = cudaMemset(ws->err, 0, sizeof(int));
+    for (auto& ev : ws->ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) {
+        ws_release(ws);
+        delete ws;
+        return cuda_fail(e, "CUDA: workspace setup failed");
+    }
+    *out = ws;
+    return OZA_OK;
+}
+
+oza_status_t oza_ws_destroy(oza_ws_t ws) {
+    if (!ws) return OZA_OK;
+    DeviceGuard g(ws->ex->device);
+    ws_release(ws);
+    delete ws;
+    return OZA_OK;
+}
+
+oza_status_t oza_ws_get_ptr(oza_ws_t ws, int which, void** ptr) {
+    if (!ws || !ptr) return fail(OZA_INVALID_ARG, "oza_ws_get_ptr: null argument");
+    switch (which) {
+        case OZA_BUF_SHIFT_A: *ptr = ws->shiftA; break;
+        case OZA_BUF_SHIFT_B: *ptr = ws->shiftB; break;
+        case OZA_BUF_A_SLICES: *ptr = ws->aplanes; break;
+        case OZA_BUF_B_SLICES: *ptr = ws->bplanes; break;
+        case OZA_BUF_C_TC: *ptr = ws->ctc; break;
+        default: return fail(OZA_INVALID_ARG, "oza_ws_get_ptr: unknown buffer %d", which);
+    }
+    return OZA_OK;
+}
+
+oza_status_t oza_ws_get_info(oza_ws_t ws, oza_ws_info_t* info) {
+    if (!ws || !info) return fail(OZA_INVALID_ARG, "oza_ws_get_info: null argument");
+    info->scheme = ws->scheme;
+    info->slices = ws->S;
+    info->M = ws->M;
+    info->N = ws->N;
+    info->K = ws->K;
+    info->Mp = ws->Mp;
+    info->Np = ws->Np;
+    info->Kp = ws->Kp;
+    info->groups = ws->groups;
+    info->k_param = ws->k_param;
+    info->beta = ws->beta;
+    info->flags = ws->flags;
+    info->bytes = ws->bytes;
+    return OZA_OK;
+}
+
+oza_status_t oza_ws_device_error(oza_ws_t ws, int* code) {
+    if (!ws || !code) return fail(OZA_INVALID_ARG, "oza_ws_device_error: null argument");
+    DeviceGuard g(ws->ex->device);
+    OZA_CUDA_TRY(cudaStreamSynchronize(ws->ex->stream), "CUDA: synchronize failed");
+    OZA_CUDA_TRY(cudaMemcpy(code, ws->err, sizeof(int), cudaMemcpyDeviceToHost), "CUDA: error word read failed");
+    return OZA_OK;
+}
+
+// ---------------------------------------------------------------- GEMM
+oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, oza_timings_t* timings) {
+    if (!ws) return fail(OZA_INVALID_ARG, "oza_gemm: null workspace");
+    if (ws->M == 0 || ws->N == 0) {
+        if (timings) std::memset(timings, 0, sizeof(*timings));
+        return OZA_OK;
+    }
+    if (!C || (ws->K && (!A || !B))) return fail(OZA_INVALID_ARG, "oza_gemm: null matrix pointer");
+    oza_executor* ex = ws->ex;
+    DeviceGuard g(ex->device);
+    if (!g.ok) return fail(OZA_CUDA_ERROR, "CUDA: Failed to set device %d", ex->device);
+    cudaStream_t st = ex->stream;
+    const size_t M = ws->M, N = ws->N, K = ws->K;
+
+    if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[0], st), "CUDA: event record");
+    if (K == 0) {
+        // Empty inner dimension: the product is exactly zero.
+        OZA_CUDA_TRY(cudaMemsetAsync(C, 0, M * N * sizeof(double), st), "CUDA: memset");
+        for (int i = 1; i < 5 && timings; ++i) OZA_CUDA_TRY(cudaEventRecord(ws->ev[i], st), "CUDA: event record");
+    } else {
+        const int offset = ws->scheme == OZA_SCHEME2 ? ws->k_param : 0;
+        // step 1
+        OZA_CUDA_TRY(oza::launch_stats_rows(A, M, K, offset, ws->shiftA, ex->sms, st), "step1 rows");
+        OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, st), "step1 cols");
+        if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[1], st), "CUDA: event record");
+        // step 2
+        OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A, M, K, ws->shiftA, ws->S, ws->beta, ws->aplanes, ws->Mp,
+                                            ws->Kp, ex->sms, st),
+                     "step2 rows");
+        OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
+                                            ws->bplanes, ws->Np, ws->Kp, st),
+                     "step2 cols");
+        if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[2], st), "CUDA: event record");
+        // step 3
+        oza::GemmPlan plan;
+        plan.a_planes = ws->aplanes;
+        plan.b_planes = ws->bplanes;
+        plan.planes = ws->S;
+        plan.Mp = ws->Mp;
+        plan.Np = ws->Np;
+        plan.Kp = ws->Kp;
+        plan.pairs = ws->pairs;
+        plan.ctc = ws->ctc;
+        plan.err = ws->err;
+        plan.sms = ex->sms;
+        OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
+        if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[3], st), "CUDA: event record");
+        // step 4
+        if (ws->scheme == OZA_SCHEME2)
+            OZA_CUDA_TRY(oza::launch_reconstruct2(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->shiftA, ws->shiftB, C, st),
+                         "step4 crt");
+        else
+            OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->beta, ws->shiftA,
+                                                  ws->shiftB, C, st),
+                         "step4 sum");
+        if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[4], st), "CUDA: event record");
+    }
+    if (timings) {
+        OZA_CUDA_TRY(cudaEventSynchronize(ws->ev[4]), "CUDA: event synchronize");
+        cudaEventElapsedTime(&timings->step1_ms, ws->ev[0], ws->ev[1]);
+        cudaEventElapsedTime(&timings->step2_ms, ws->ev[1], ws->ev[2]);
+        cudaEventElapsedTime(&timings->step3_ms, ws->ev[2], ws->ev[3]);
+        cudaEventElapsedTime(&timings->step4_ms, ws->ev[3], ws->ev[4]);
+        cudaEventElapsedTime(&timings->total_ms, ws->ev[0], ws->ev[4]);
+        int code = 0;
+        OZA_CUDA_TRY(cudaMemcpy(&code, ws->err, sizeof(int), cudaMemcpyDeviceToHost), "CUDA: error word read");
+        if (code) return fail(OZA_TIMEOUT, "OzaBLAS: a device-side wait expired (code %d)", code);
+    }
+    return OZA_OK;
+}
+
+// ---------------------------------------------------------------- host utilities
+oza_status_t oza_generate_matrix(int rows, int cols, double phi, int seed, double* out) {
+    if (rows < 0 || cols < 0 || (!out && rows && cols)) return fail(OZA_INVALID_ARG, "oza_generate_matrix: bad argument");
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<double> unif(0.0, 1.0);
+    std::normal_distribution<double> norm(0.0, 1.0);
+    const size_t n = (size_t)rows * (size_t)cols;
+    for (size_t i = 0; i < n; ++i) {
+        const double u = 1.0 - unif(rng);   // (0, 1]
+        const double g = norm(rng);
+        out[i] = (u - 0.5) * std::exp(phi * g);
+    }
+    return OZA_OK;
+}
+
+int oza_scheme1_beta(size_t K) {
+    int beta = (int)std::floor((31.0 - std::log2((double)K)) / 2.0);
+    return beta < 1 ? 1 : (beta > 7 ? 7 : beta);
+}
+
+int oza_scheme2_k_param(int slices, size_t K) {
+    if (slices < 1 || slices > 20 || K == 0) return 0;
+    // M = prod of the first S moduli, converted to double through 64-bit limbs
+    // and a left-to-right sum as the reference does (crt_math.hpp:73-80).
+    static const unsigned mod[20] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
+                                     193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
+    uint64_t w[4] = {1, 0, 0, 0};
+    for (int i = 0; i < slices; ++i) {
+        unsigned __int128 carry = 0;
+        for (int l = 0; l < 4; ++l) {
+            unsigned __int128 p = (unsigned __int128)w[l] * mod[i] + carry;
+            w[l] = (uint64_t)p;
+            carry = p >> 64;
+        }
+    }
+    double Md = 0.0;
+    Md += (double)w[0];
+    Md += std::ldexp((double)w[1], 64);
+    Md += std::ldexp((double)w[2], 128);
+    Md += std::ldexp((double)w[3], 192);
+    double frac = (Md / 2.0 - 1.0) / (double)K;
+    return (int)std::floor(0.5 * std::log2(frac));
+}
+
+}  // extern "C"

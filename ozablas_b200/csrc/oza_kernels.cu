@@ -1,0 +1,961 @@
+// oza_kernels.cu -- sm_100a kernels of the Ozaki Scheme I / II FP64 GEMM.
+//
+//   step 1  k_stats_rows / k_stats_cols      max frexp exponent per row of A /
+//                                            column of B (warp reductions over
+//                                            coalesced loads)
+//   step 2  k_slice_rows / k_slice_cols      INT8 slices (Scheme I) or symmetric
+//                                            residues (Scheme II) written as
+//                                            K-major, zero-padded planes
+//   step 3  k_gemm_i8                        persistent warp-specialised
+//                                            tcgen05 kind::i8 GEMM: TMA ->
+//                                            128B-swizzled smem ring -> UMMA ->
+//                                            INT32 accumulators in TMEM (double
+//                                            buffered) -> epilogue warps
+//   step 4  k_reconstruct2 / k_reconstruct1  exact CRT reconstruction (II) and
+//                                            scaled group sum (I)
+//
+// Parity: every stage reproduces the reference pipeline bit for bit
+// (src/pipeline/step1_statistics.hpp, step2_slicing.hpp,
+// step4_reconstruction.hpp, src/cuda/pipeline.cu of IlyaNyrkov/ozablas); the
+// tests compare each intermediate with the CPU oracle.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "oza_device.cuh"
+#include "oza_kernels.h"
+
+namespace oza {
+
+__constant__ ModConst c_mod[kMaxSlices];
+__constant__ CrtTable c_crt[kMaxSlices];
+
+// The reference's moduli (src/common/crt_tables.hpp:13-16).  The residues are
+// only comparable with the same list in the same order.
+static const uint32_t kModuli[kMaxSlices] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
+                                             193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
+
+// ---------------------------------------------------------------------------
+// Host: constant tables
+// ---------------------------------------------------------------------------
+namespace {
+
+// Little-endian multiword integer with 32-bit limbs.
+struct Big {
+    uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+Big big_from(uint32_t v) {
+    Big b;
+    b.w[0] = v;
+    return b;
+}
+
+Big big_mul_small(const Big& a, uint32_t m) {
+    Big r;
+    uint64_t carry = 0;
+    for (int i = 0; i < 8; ++i) {
+        uint64_t p = (uint64_t)a.w[i] * m + carry;
+        r.w[i] = (uint32_t)p;
+        carry = p >> 32;
+    }
+    return r;
+}
+
+uint32_t big_mod_small(const Big& a, uint32_t m) {
+    uint64_t rem = 0;
+    for (int i = 7; i >= 0; --i) rem = ((rem << 32) | a.w[i]) % m;
+    return (uint32_t)rem;
+}
+
+int32_t sym_rep(uint32_t r, uint32_t m) { return r > m / 2 ? (int32_t)r - (int32_t)m : (int32_t)r; }
+
+uint32_t pow2_mod(int e, uint32_t m) {
+    uint64_t r = 1 % m;
+    for (int i = 0; i < e; ++i) r = (r * 2) % m;
+    return (uint32_t)r;
+}
+
+std::mutex g_table_mu;
+uint64_t g_table_done = 0;   // bit per device ordinal
+
+}  // namespace
+
+cudaError_t upload_tables() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    if (dev < 64 && (g_table_done >> dev) & 1ull) return cudaSuccess;
+
+    static ModConst mc[kMaxSlices];
+    static CrtTable ct[kMaxSlices];
+    for (int s = 0; s < kMaxSlices; ++s) {
+        uint32_t m = kModuli[s];
+        mc[s].m = m;
+        mc[s].magic = (uint32_t)(((1ull << 39) + m - 1) / m);
+        mc[s].c21 = sym_rep(pow2_mod(21, m), m);
+        mc[s].c42 = sym_rep(pow2_mod(42, m), m);
+        mc[s].c63 = sym_rep(pow2_mod(63, m), m);
+        mc[s].pad = 0;
+    }
+    for (int S = 1; S <= kMaxSlices; ++S) {
+        CrtTable& t = ct[S - 1];
+        Big M = big_from(1);
+        for (int i = 0; i < S; ++i) M = big_mul_small(M, kModuli[i]);
+        for (int l = 0; l < 5; ++l) {
+            t.M[l] = M.w[l];
+            t.Mhalf[l] = (M.w[l] >> 1) | (M.w[l + 1] << 31);
+        }
+        int nl = 1;
+        for (int l = 0; l < 5; ++l)
+            if (M.w[l]) nl = l + 1;
+        t.nlimbs = nl;
+        for (int i = 0; i < kMaxSlices; ++i) {
+            if (i >= S) {
+                for (int l = 0; l < 5; ++l) t.P[i][l] = 0;
+                t.inv[i] = 0;
+                t.c16inv[i] = 0;
+                t.recip[i] = 0.f;
+                continue;
+            }
+            Big P = big_from(1);
+            for (int j = 0; j < S; ++j)
+                if (j != i) P = big_mul_small(P, kModuli[j]);
+            for (int l = 0; l < 5; ++l) t.P[i][l] = P.w[l];
+            uint32_t m = kModuli[i], r = big_mod_small(P, m), inv = 0;
+            for (uint32_t c = 1; c < m; ++c)
+                if ((uint64_t)r * c % m == 1) {
+                    inv = c;
+                    break;
+                }
+            t.inv[i] = inv;
+            t.c16inv[i] = (uint32_t)((65536ull * inv) % m);
+            t.recip[i] = 1.0f / (float)m;
+        }
+    }
+    e = cudaMemcpyToSymbol(c_mod, mc, sizeof(mc));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_crt, ct, sizeof(ct));
+    if (e != cudaSuccess) return e;
+    if (dev < 64) g_table_done |= 1ull << dev;
+    return cudaSuccess;
+}
+
+PairList make_pairs(int scheme, int slices) {
+    PairList p{};
+    int n = 0;
+    p.num_groups = slices;
+    for (int g = 0; g < slices; ++g) {
+        p.start[g] = n;
+        if (scheme == 2) {
+            p.a[n] = (uint8_t)g;
+            p.b[n] = (uint8_t)g;
+            ++n;
+        } else {
+            // group g+2 (1-based slices s + t = g + 2), reference pipeline.cu:102-126
+            int G = g + 2;
+            for (int s = 1; s <= G - 1; ++s) {
+                int t = G - s;
+                if (s > slices || t > slices) continue;
+                p.a[n] = (uint8_t)(s - 1);
+                p.b[n] = (uint8_t)(t - 1);
+                ++n;
+            }
+        }
+    }
+    p.start[slices] = n;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Step 1: exponent statistics
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kMagMask = 0x7FFFFFFFFFFFFFFFull;
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+// One warp per row of A: shift[r] = offset - max frexp exponent (-1023 for an
+// all-zero row).  Reference: compute_row_shifts_A, step1_statistics.hpp:23-76.
+// The maximum exponent is taken from the maximum magnitude bit pattern, which
+// orders like |x| for finite doubles.
+__global__ void __launch_bounds__(256) k_stats_rows(const double* __restrict__ A, long long rows, long long cols,
+                                                    int offset, int32_t* __restrict__ shift, bool vec2) {
+    const int lane = threadIdx.x & 31;
+    const long long warps_total = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+         r += warps_total) {
+        const double* row = A + r * cols;
+        unsigned long long mx = 0;
+        if (vec2) {
+            const double2* row2 = reinterpret_cast<const double2*>(row);
+            long long n2 = cols >> 1;
+            for (long long k = lane; k < n2; k += 32) {
+                double2 v = __ldg(row2 + k);
+                unsigned long long a = (unsigned long long)__double_as_longlong(v.x) & kMagMask;
+                unsigned long long b = (unsigned long long)__double_as_longlong(v.y) & kMagMask;
+                mx = a > mx ? a : mx;
+                mx = b > mx ? b : mx;
+            }
+            if ((cols & 1) && lane == 0) {
+                unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + cols - 1)) & kMagMask;
+                mx = a > mx ? a : mx;
+            }
+        } else {
+            for (long long k = lane; k < cols; k += 32) {
+                unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + k)) & kMagMask;
+                mx = a > mx ? a : mx;
+            }
+        }
+        mx = warp_max_u64(mx);
+        if (lane == 0) shift[r] = offset - max_exp_from_bits(mx);
+    }
+}
+
+// Column maxima of B (K x N) as magnitude bits, combined with atomicMax into
+// colmax[] (zeroed beforehand; 0 encodes an all-zero column).  Block: 8 warps
+// over a 64-column strip, each lane owning 2 adjacent columns; grid.y splits
+// the rows.  Reference: compute_col_shifts_B, step1_statistics.hpp:78-99.
+__global__ void __launch_bounds__(256) k_stats_cols(const double* __restrict__ B, long long rows, long long cols,
+                                                    unsigned long long* __restrict__ colmax) {
+    __shared__ unsigned long long part[8][64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long c0 = (long long)blockIdx.x * 64 + 2 * lane;
+    unsigned long long m0 = 0, m1 = 0;
+    for (long long r = (long long)blockIdx.y * 8 + warp; r < rows; r += (long long)gridDim.y * 8) {
+        const double* row = B + r * cols;
+        if (c0 < cols) {
+            unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + c0)) & kMagMask;
+            m0 = a > m0 ? a : m0;
+        }
+        if (c0 + 1 < cols) {
+            unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + c0 + 1)) & kMagMask;
+            m1 = a > m1 ? a : m1;
+        }
+    }
+    part[warp][2 * lane] = m0;
+    part[warp][2 * lane + 1] = m1;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        unsigned long long m = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) m = part[w][threadIdx.x] > m ? part[w][threadIdx.x] : m;
+        long long c = (long long)blockIdx.x * 64 + threadIdx.x;
+        if (c < cols && m != 0) atomicMax(colmax + c, m);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Step 2: slicing
+// ---------------------------------------------------------------------------
+
+// x * 2^sh exactly as ldexp rounds it.  A multiplication by an exact power of
+// two rounds the same way; outside the normal exponent range fall back.
+__device__ __forceinline__ double scale_pow2(double x, int sh, double p) {
+    return (sh >= -1022 && sh <= 1023) ? x * p : ldexp(x, sh);
+}
+
+__device__ __forceinline__ double pow2_or_zero(int sh) {
+    return (sh >= -1022 && sh <= 1023) ? __longlong_as_double((long long)(sh + 1023) << 52) : 0.0;
+}
+
+// Radix-2^21 split of an integer-valued double |x| < 2^84 into int32 digits.
+template <bool FOUR>
+__device__ __forceinline__ void split21(double x, int& d0, int& d1, int& d2, int& d3) {
+    double r = x;
+    if (FOUR) {
+        double q3 = rint(r * 0x1p-63);
+        r = r - q3 * 0x1p63;
+        d3 = __double2int_rn(q3);
+    } else {
+        d3 = 0;
+    }
+    double q2 = rint(r * 0x1p-42);
+    r = r - q2 * 0x1p42;
+    double q1 = rint(r * 0x1p-21);
+    r = r - q1 * 0x1p21;
+    d2 = __double2int_rn(q2);
+    d1 = __double2int_rn(q1);
+    d0 = __double2int_rn(r);
+}
+
+// Symmetric residue in [-(m-1)/2, (m-1)/2] of the integer with digits d (radix
+// 2^21), modulo c_mod[s].m.  y = sum d_i * (2^(21 i) mod m) stays below 2^29
+// in magnitude, the bias m * 2^22 makes it positive and below 2^31, and the
+// magic-number division is exact there.
+template <bool FOUR>
+__device__ __forceinline__ int symmetric_residue(int s, int d0, int d1, int d2, int d3) {
+    const ModConst mc = c_mod[s];
+    int y = d0 + d1 * mc.c21 + d2 * mc.c42;
+    if (FOUR) y += d3 * mc.c63;
+    uint32_t u = (uint32_t)(y + (int)(mc.m << 22));
+    uint32_t r = u - div_small(u, mc.magic) * mc.m;
+    return (int)r - ((r > (mc.m >> 1)) ? (int)mc.m : 0);
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+    return (uint32_t)(a & 0xFF) | ((uint32_t)(b & 0xFF) << 8) | ((uint32_t)(c & 0xFF) << 16) |
+           ((uint32_t)(d & 0xFF) << 24);
+}
+
+// double -> int8 as the sm_100 conversion does it: truncate, saturate, NaN -> 0.
+__device__ __forceinline__ int cvt_s8(double v) {
+    int i = __double2int_rz(v);
+    return i > 127 ? 127 : (i < -128 ? -128 : i);
+}
+
+// Scheme II residues of 16 consecutive values.  out16[s] receives the packed bytes.
+template <bool FOUR>
+__device__ __forceinline__ void residues16(const double (&v)[16], int sh, double p, int S, uint4* dst,
+                                           size_t plane_stride) {
+    int d0[16], d1[16], d2[16], d3[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        double x = rint(scale_pow2(v[i], sh, p));
+        split21<FOUR>(x, d0[i], d1[i], d2[i], d3[i]);
+    }
+    for (int s = 0; s < S; ++s) {
+        int r[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) r[i] = symmetric_residue<FOUR>(s, d0[i], d1[i], d2[i], d3[i]);
+        uint4 o;
+        o.x = pack4(r[0], r[1], r[2], r[3]);
+        o.y = pack4(r[4], r[5], r[6], r[7]);
+        o.z = pack4(r[8], r[9], r[10], r[11]);
+        o.w = pack4(r[12], r[13], r[14], r[15]);
+        *reinterpret_cast<uint4*>(reinterpret_cast<int8_t*>(dst) + (size_t)s * plane_stride) = o;
+    }
+}
+
+// Scheme I slices of 16 consecutive values of one row/column with max exponent
+// e (reference slice_scheme1_A/B, step2_slicing.hpp:44-100).
+__device__ __forceinline__ void slices16(const double (&vin)[16], int e, int beta, int S, uint4* dst,
+                                         size_t plane_stride) {
+    const double scale = ldexp(1.0, e + 1 - beta);
+    const double inv_scale = ldexp(1.0, -(e + 1 - beta));
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = vin[i];
+    for (int s = 0; s < S; ++s) {
+        const double sigma = 0.75 * ldexp(scale, 53 - beta * s);
+        const double up = ldexp(1.0, beta * s);   // exact: slice values are small integers
+        int r[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            double vs = __dsub_rn(__dadd_rn(v[i], sigma), sigma);
+            double sl = __dmul_rn(__dmul_rn(vs, inv_scale), up);
+            r[i] = cvt_s8(sl);
+            v[i] = __dsub_rn(v[i], vs);
+        }
+        uint4 o;
+        o.x = pack4(r[0], r[1], r[2], r[3]);
+        o.y = pack4(r[4], r[5], r[6], r[7]);
+        o.z = pack4(r[8], r[9], r[10], r[11]);
+        o.w = pack4(r[12], r[13], r[14], r[15]);
+        *reinterpret_cast<uint4*>(reinterpret_cast<int8_t*>(dst) + (size_t)s * plane_stride) = o;
+    }
+}
+
+// A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per 16
+// consecutive columns of a row (16-byte stores per plane, coalesced).
+template <int SCHEME, bool FOUR>
+__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long long rows, long long cols,
+                                                    const int32_t* __restrict__ shift, int S, int beta,
+                                                    int8_t* __restrict__ out, long long rows_p, long long cols_p) {
+    const long long chunks_per_row = cols_p >> 4;
+    const long long total = rows_p * chunks_per_row;
+    const size_t plane = (size_t)rows_p * (size_t)cols_p;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const long long r = id / chunks_per_row;
+        const long long c0 = (id - r * chunks_per_row) << 4;
+        double v[16];
+        int sh = 0;
+        if (r < rows) {
+            sh = shift[r];
+            const double* src = A + r * cols + c0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = 0.0;
+        }
+        uint4* dst = reinterpret_cast<uint4*>(out + (size_t)r * cols_p + c0);
+        if (SCHEME == 2) {
+            residues16<FOUR>(v, sh, pow2_or_zero(sh), S, dst, plane);
+        } else {
+            slices16(v, r < rows ? -sh : -1023, beta, S, dst, plane);
+        }
+    }
+}
+
+// B (K x N, row-major) -> out[s][Np][Kp], i.e. B^T, K-major.  Tile of 128 k x
+// 32 n staged through shared memory; thread (n, kg) emits 16 consecutive k of
+// column n.  Also writes shift[n] = offset - max exponent of column n.
+template <int SCHEME, bool FOUR>
+__global__ void __launch_bounds__(256) k_slice_cols(const double* __restrict__ B, long long K, long long N,
+                                                    const unsigned long long* __restrict__ colmax, int offset,
+                                                    int S, int beta, int32_t* __restrict__ shift,
+                                                    int8_t* __restrict__ out, long long Np, long long Kp) {
+    __shared__ double tile[128][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long n0 = (long long)blockIdx.x * 32, k0 = (long long)blockIdx.y * 128;
+    // Load: warp w reads rows k0 + w + 8 i, 32 consecutive columns.
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        long long k = k0 + warp + 8 * i, n = n0 + lane;
+        tile[warp + 8 * i][lane] = (k < K && n < N) ? __ldg(B + k * N + n) : 0.0;
+    }
+    __syncthreads();
+    const long long n = n0 + lane;
+    const int kg = warp;   // 16-row group
+    int e = (n < N) ? max_exp_from_bits(colmax[n]) : -1023;
+    int sh = offset - e;
+    if (blockIdx.y == 0 && kg == 0 && n < N) shift[n] = sh;
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = tile[kg * 16 + i][lane];
+    const size_t plane = (size_t)Np * (size_t)Kp;
+    uint4* dst = reinterpret_cast<uint4*>(out + (size_t)n * Kp + k0 + kg * 16);
+    if (SCHEME == 2) {
+        residues16<FOUR>(v, sh, pow2_or_zero(sh), S, dst, plane);
+    } else {
+        slices16(v, e, beta, S, dst, plane);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Step 3: tcgen05 INT8 GEMM
+// ---------------------------------------------------------------------------
+constexpr int kGemmThreads = 192;   // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kStages = 4;
+constexpr int kABytes = kTileM * kTileK;   // 16 KB per stage
+constexpr int kBBytes = kTileN * kTileK;   // 32 KB per stage
+constexpr uint32_t kAccCols = kTileN;      // TMEM columns per accumulator
+constexpr uint32_t kTmemCols = 2 * kAccCols;
+constexpr int kGemmSmem = kStages * (kABytes + kBBytes) + 1024 /*align*/ + 256 /*barriers*/;
+
+struct GemmArgs {
+    int m_tiles, n_tiles, k_blocks, total_tiles;
+    long long Mp, Np;
+    int32_t* ctc;
+    int* err;
+};
+
+__device__ __forceinline__ void decode_tile(int t, const GemmArgs& g, int& grp, int& mt, int& nt) {
+    const int per = g.m_tiles * g.n_tiles;
+    grp = t / per;
+    const int rem = t - grp * per;
+    mt = rem / g.n_tiles;
+    nt = rem - mt * g.n_tiles;
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              const __grid_constant__ PairList pairs, const GemmArgs args) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + kStages * kABytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + kStages * kBBytes);
+    uint64_t* empty = full + kStages;
+    uint64_t* acc_full = empty + kStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&acc_full[0], 1);
+        mbar_init(&acc_full[1], 1);
+        mbar_init(&acc_empty[0], 4);
+        mbar_init(&acc_empty[1], 4);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        int stage = 0;
+        uint32_t phase = 0;
+        long long issued = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+            int grp, mt, nt;
+            decode_tile(t, args, grp, mt, nt);
+            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kTileM);
+                const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN);
+                for (int kb = 0; kb < args.k_blocks; ++kb) {
+                    int w = 1;
+                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
+                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                    if (!ok) break;
+                    if (lane == 0) {
+                        mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
+                        tma_load_2d(sA + stage * kABytes, &tmA, &full[stage], kb * kTileK, arow);
+                        tma_load_2d(sB + stage * kBBytes, &tmB, &full[stage], kb * kTileK, brow);
+                    }
+                    __syncwarp();
+                    ++issued;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+        }
+        if (!ok && lane == 0) {
+            // Let the copies already issued land before the CTA leaves.
+            long long n = issued < kStages ? issued : kStages;
+            volatile int no_abort = 0;
+            for (long long j = 0; j < n; ++j) {
+                long long idx = issued - 1 - j;
+                mbar_wait(&full[idx % kStages], (uint32_t)((idx / kStages) & 1), &no_abort, nullptr);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        constexpr uint32_t idesc = umma_idesc_i8(kTileM, kTileN);
+        int stage = 0;
+        uint32_t phase = 0;
+        int local = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x, ++local) {
+            int grp, mt, nt;
+            decode_tile(t, args, grp, mt, nt);
+            const int acc = local & 1;
+            const uint32_t acc_phase = (local >> 1) & 1;
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
+            ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t d = tmem_base + acc * kAccCols;
+            uint32_t accumulate = 0;
+            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                for (int kb = 0; kb < args.k_blocks; ++kb) {
+                    w = 1;
+                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
+                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                    if (!ok) break;
+                    tc_fence_after();
+                    if (lane == 0) {
+                        const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
+                        const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
+#pragma unroll
+                        for (int k = 0; k < kTileK / 32; ++k) {
+                            // +32 bytes of K inside the swizzle row = +2 in 16-byte units
+                            umma_i8(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
+                            accumulate = 1;
+                        }
+                        umma_commit(&empty[stage]);
+                    }
+                    __syncwarp();
+                    accumulate = 1;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (!ok) break;
+            if (lane == 0) umma_commit(&acc_full[acc]);
+            __syncwarp();
+        }
+        if (!ok && lane == 0) {
+            // Wait for the MMAs already issued before TMEM is released.
+            umma_commit(drain);
+            volatile int no_abort = 0;
+            mbar_wait(drain, 0, &no_abort, nullptr);
+        }
+    } else {
+        // ---------------- epilogue: TMEM -> INT32 planes ----------------
+        const int q = warp & 3;   // TMEM lane quadrant this warp may access
+        int local = 0;
+        for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x, ++local) {
+            int grp, mt, nt;
+            decode_tile(t, args, grp, mt, nt);
+            const int acc = local & 1;
+            const uint32_t acc_phase = (local >> 1) & 1;
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
+            if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) break;
+            tc_fence_after();
+            const long long row = (long long)mt * kTileM + q * 32 + lane;
+            int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np + (size_t)nt * kTileN;
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols;
+#pragma unroll 1
+            for (int c = 0; c < kTileN / 32; ++c) {
+                uint32_t r[32];
+                tmem_ld32(taddr + c * 32, r);
+                tmem_ld_wait();
+                int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+#pragma unroll
+                for (int v = 0; v < 8; ++v)
+                    d4[v] = make_int4((int)r[4 * v], (int)r[4 * v + 1], (int)r[4 * v + 2], (int)r[4 * v + 3]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, kTmemCols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Step 4: reconstruction
+// ---------------------------------------------------------------------------
+
+// (C * inv_s) mod m_s in [0, m_s) for any int32 C: C = hi * 2^16 + lo,
+// y = hi * ((2^16 inv) mod m) + lo * inv + m * 2^16 lies in (0, 2^31).
+__device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t magic, uint32_t inv,
+                                              uint32_t c16inv) {
+    const int hi = C >> 16;
+    const int lo = C & 0xFFFF;
+    const uint32_t u = (uint32_t)(hi * (int)c16inv + lo * (int)inv + (int)(m << 16));
+    return u - div_small(u, magic) * m;
+}
+
+// Exact CRT reconstruction of one element from its S INT32 products, then the
+// reference's conversion (step4_reconstruction.hpp:59-184, crt_math.hpp:73-80):
+// T = sum c_s * (M/m_s); x = T mod M; if x >= floor(M/2) the value is -(M-x);
+// magnitude to double as d0 + d1 2^64 + d2 2^128 (64-bit limbs, rounding after
+// each add); finally ldexp(., -(shift_A + shift_B)).
+template <int NL>
+__device__ __forceinline__ double crt_to_double(const int32_t* vals, int S, int esum) {
+    const CrtTable& T = c_crt[S - 1];
+    unsigned long long acc[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) acc[l] = 0ull;
+    float qf = 0.f;
+    for (int s = 0; s < S; ++s) {
+        const uint32_t m = c_mod[s].m;
+        const uint32_t c = crt_coeff(vals[s], m, c_mod[s].magic, T.inv[s], T.c16inv[s]);
+#pragma unroll
+        for (int l = 0; l < NL; ++l) acc[l] += (unsigned long long)c * T.P[s][l];
+        qf = fmaf((float)c, T.recip[s], qf);
+    }
+    // carry-normalise T into NL+1 32-bit limbs
+    uint32_t t[NL + 1];
+    unsigned long long carry = 0;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        unsigned long long v = acc[l] + carry;
+        t[l] = (uint32_t)v;
+        carry = v >> 32;
+    }
+    t[NL] = (uint32_t)carry;
+    // R = T - q M with q = floor(T / M) estimated in float (|error| < 1), then one fix-up.
+    const uint32_t q = (uint32_t)floorf(qf);
+    long long borrow = 0;
+    uint32_t r[NL + 1];
+    {
+        unsigned long long qc = 0;
+#pragma unroll
+        for (int l = 0; l <= NL; ++l) {
+            unsigned long long qm = (unsigned long long)q * (l < NL ? T.M[l] : 0u) + qc;
+            qc = qm >> 32;
+            long long d = (long long)t[l] - (long long)(uint32_t)qm - borrow;
+            borrow = d < 0 ? 1 : 0;
+            r[l] = (uint32_t)d;
+        }
+    }
+    if (borrow) {   // estimate one too large: R += M
+        unsigned long long c = 0;
+#pragma unroll
+        for (int l = 0; l <= NL; ++l) {
+            unsigned long long v = (unsigned long long)r[l] + (l < NL ? T.M[l] : 0u) + c;
+            r[l] = (uint32_t)v;
+            c = v >> 32;
+        }
+    } else {
+        // R >= M ?  then R -= M
+        bool ge = true;
+        if (r[NL] != 0) {
+            ge = true;
+        } else {
+#pragma unroll
+            for (int l = NL - 1; l >= 0; --l) {
+                if (r[l] != T.M[l]) {
+                    ge = r[l] > T.M[l];
+                    break;
+                }
+            }
+        }
+        if (ge) {
+            long long b = 0;
+#pragma unroll
+            for (int l = 0; l <= NL; ++l) {
+                long long d = (long long)r[l] - (long long)(l < NL ? T.M[l] : 0u) - b;
+                b = d < 0 ? 1 : 0;
+                r[l] = (uint32_t)d;
+            }
+        }
+    }
+    // signed map at floor(M/2)
+    bool neg = true;
+#pragma unroll
+    for (int l = NL - 1; l >= 0; --l) {
+        if (r[l] != T.Mhalf[l]) {
+            neg = r[l] > T.Mhalf[l];
+            break;
+        }
+    }
+    if (neg) {
+        long long b = 0;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            long long d = (long long)T.M[l] - (long long)r[l] - b;
+            b = d < 0 ? 1 : 0;
+            r[l] = (uint32_t)d;
+        }
+    }
+    // 4-limb (64-bit) sum as the reference converts it
+    double mag = 0.0;
+    mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)r[0] | (NL > 1 ? (unsigned long long)r[1] << 32 : 0ull)));
+    if (NL > 2) {
+        unsigned long long w1 = (unsigned long long)r[2] | (NL > 3 ? (unsigned long long)r[3] << 32 : 0ull);
+        mag = __dadd_rn(mag, __ull2double_rn(w1) * 0x1p64);
+    }
+    if (NL > 4) {
+        unsigned long long w2 = (unsigned long long)r[4];
+        mag = __dadd_rn(mag, __ull2double_rn(w2) * 0x1p128);
+    }
+    return ldexp(neg ? -mag : mag, -esum);
+}
+
+template <int NL>
+__global__ void __launch_bounds__(256) k_reconstruct2(const int32_t* __restrict__ ctc, long long Mp, long long Np,
+                                                      long long M, long long N, int S,
+                                                      const int32_t* __restrict__ sA,
+                                                      const int32_t* __restrict__ sB, double* __restrict__ C) {
+    const long long total = M * N;
+    const size_t plane = (size_t)Mp * (size_t)Np;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const long long i = id / N, j = id - i * N;
+        int32_t vals[kMaxSlices];
+        const int32_t* src = ctc + (size_t)i * Np + j;
+#pragma unroll
+        for (int s = 0; s < kMaxSlices; ++s)
+            if (s < S) vals[s] = __ldg(src + (size_t)s * plane);
+        C[id] = crt_to_double<NL>(vals, S, sA[i] + sB[j]);
+    }
+}
+
+// Scheme I: C = sum over g = 2..S+1 (in that order) of double(C_g) * scale_g,
+// each update one fused multiply-add from +0.0, which is the sequence of the
+// reference's per-group launches (step4_reconstruction.hpp:21-49,
+// pipeline.cu:102-135 after the memset at pipeline.cu:72).
+__global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict__ ctc, long long Mp, long long Np,
+                                                      long long M, long long N, int S, int beta,
+                                                      const int32_t* __restrict__ negA,
+                                                      const int32_t* __restrict__ negB, double* __restrict__ C) {
+    const long long total = M * N;
+    const size_t plane = (size_t)Mp * (size_t)Np;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const long long i = id / N, j = id - i * N;
+        const double ui = ldexp(1.0, -negA[i] + 1 - beta);
+        const double vj = ldexp(1.0, -negB[j] + 1 - beta);
+        const double uv = __dmul_rn(ui, vj);
+        const int32_t* src = ctc + (size_t)i * Np + j;
+        double acc = 0.0;
+        for (int g = 2; g <= S + 1; ++g) {
+            const double scale = ldexp(uv, -beta * g + 2 * beta);
+            acc = __fma_rn((double)__ldg(src + (size_t)(g - 2) * plane), scale, acc);
+        }
+        C[id] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+namespace {
+
+int grid_for(long long work, int per_block, int sms, int waves = 8) {
+    long long b = (work + per_block - 1) / per_block;
+    long long cap = (long long)sms * waves;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// K-major int8 planes [rows][Kp] as a 2D tensor with a (128 x box_rows) box
+// and the 128-byte swizzle the UMMA descriptors expect.
+bool make_plane_map(CUtensorMap* map, const int8_t* base, size_t rows, size_t Kp, int box_rows) {
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)Kp};
+    cuuint32_t box[2] = {(cuuint32_t)kTileK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+cudaError_t launch_stats_rows(const double* A, size_t rows, size_t cols, int offset, int32_t* shift, int sms,
+                              cudaStream_t st) {
+    if (rows == 0) return cudaSuccess;
+    bool vec2 = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (cols % 2 == 0);
+    int grid = grid_for((long long)rows, 8, sms);
+    k_stats_rows<<<grid, 256, 0, st>>>(A, (long long)rows, (long long)cols, offset, shift, vec2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigned long long* colmax, int sms,
+                              cudaStream_t st) {
+    if (cols == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(colmax, 0, cols * sizeof(unsigned long long), st);
+    if (e != cudaSuccess || rows == 0) return e;
+    int gx = (int)((cols + 63) / 64);
+    long long want = (long long)sms * 4 / gx;
+    long long maxy = ((long long)rows + 63) / 64;
+    int gy = (int)(want < 1 ? 1 : (want > maxy ? maxy : want));
+    if (gy < 1) gy = 1;
+    k_stats_cols<<<dim3(gx, gy), 256, 0, st>>>(B, (long long)rows, (long long)cols, colmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift, int S,
+                              int beta, int8_t* out, size_t rows_p, size_t cols_p, int sms, cudaStream_t st) {
+    long long chunks = (long long)rows_p * (long long)(cols_p / 16);
+    if (chunks == 0) return cudaSuccess;
+    int grid = grid_for(chunks, 256, sms);
+    if (scheme == 2) {
+        // rint(ldexp(x, shift)) is below 2^(K_param) in magnitude; four radix-2^21
+        // digits are needed only once K_param exceeds 62.
+        k_slice_rows<2, true><<<grid, 256, 0, st>>>(A, (long long)rows, (long long)cols, shift, S, 0, out,
+                                                    (long long)rows_p, (long long)cols_p);
+    } else {
+        k_slice_rows<1, false><<<grid, 256, 0, st>>>(A, (long long)rows, (long long)cols, shift, S, beta, out,
+                                                     (long long)rows_p, (long long)cols_p);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
+                              int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
+                              cudaStream_t st) {
+    if (Np == 0 || Kp == 0) return cudaSuccess;
+    dim3 grid((unsigned)(Np / 32), (unsigned)(Kp / 128));
+    if (scheme == 2) {
+        k_slice_cols<2, true><<<grid, 256, 0, st>>>(B, (long long)K, (long long)N, colmax, offset, S, 0, shift, out,
+                                                    (long long)Np, (long long)Kp);
+    } else {
+        k_slice_cols<1, false><<<grid, 256, 0, st>>>(B, (long long)K, (long long)N, colmax, offset, S, beta, shift,
+                                                     out, (long long)Np, (long long)Kp);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    CUtensorMap tmA, tmB;
+    if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, kTileM)) return cudaErrorInvalidValue;
+    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, kTileN)) return cudaErrorInvalidValue;
+    GemmArgs a;
+    a.m_tiles = (int)(p.Mp / kTileM);
+    a.n_tiles = (int)(p.Np / kTileN);
+    a.k_blocks = (int)(p.Kp / kTileK);
+    a.total_tiles = a.m_tiles * a.n_tiles * p.pairs.num_groups;
+    a.Mp = (long long)p.Mp;
+    a.Np = (long long)p.Np;
+    a.ctc = p.ctc;
+    a.err = p.err;
+    if (a.total_tiles == 0) return cudaSuccess;
+    int grid = a.total_tiles < p.sms ? a.total_tiles : p.sms;
+    k_gemm_i8<<<grid, kGemmThreads, kGemmSmem, st>>>(tmA, tmB, p.pairs, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S,
+                                const int32_t* shiftA, const int32_t* shiftB, double* C, cudaStream_t st) {
+    long long total = (long long)M * (long long)N;
+    if (total == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int grid = grid_for(total, 256, sms, 16);
+    // limbs of M: S <= 4 -> 1, <= 8 -> 2, <= 12 -> 3, <= 16 -> 4, else 5
+    int nl = (S + 3) / 4;
+    switch (nl) {
+        case 1: k_reconstruct2<1><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 2: k_reconstruct2<2><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 3: k_reconstruct2<3><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 4: k_reconstruct2<4><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        default: k_reconstruct2<5><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
+                                const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st) {
+    long long total = (long long)M * (long long)N;
+    if (total == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int grid = grid_for(total, 256, sms, 16);
+    k_reconstruct1<<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, beta, negA, negB, C);
+    return cudaGetLastError();
+}
+
+}  // namespace oza

@@ -1,0 +1,72 @@
+// oza_kernels.h -- host-side launch wrappers of the sm_100a kernels
+// (internal to liboza_b200; the public boundary is include/oza_capi.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace oza {
+
+constexpr int kMaxSlicesHost = 20;
+
+// Tile geometry of the INT8 tensor-core GEMM and the padding it imposes on
+// the workspace layouts.
+constexpr int kTileM = 128;   // rows of A per CTA tile (UMMA M)
+constexpr int kTileN = 256;   // rows of B^T per CTA tile (UMMA N)
+constexpr int kTileK = 128;   // bytes of K per pipeline stage (one 128B swizzle row)
+
+inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+// Which (A-plane, B-plane) products are summed into each INT32 group.
+// Scheme II: group s = A_s * B_s.  Scheme I: group g (plane g-2) sums
+// A_s * B_t over s + t = g (1-based slice indices), s, t <= S.
+struct PairList {
+    int num_groups;
+    int start[kMaxSlicesHost + 1];
+    uint8_t a[kMaxSlicesHost * (kMaxSlicesHost + 1) / 2];
+    uint8_t b[kMaxSlicesHost * (kMaxSlicesHost + 1) / 2];
+};
+PairList make_pairs(int scheme, int slices);
+
+// Upload the per-modulus and CRT constants to the current device.
+cudaError_t upload_tables();
+
+// Step 1.
+cudaError_t launch_stats_rows(const double* A, size_t rows, size_t cols, int offset, int32_t* shift,
+                              int sms, cudaStream_t st);
+cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigned long long* colmax, int sms,
+                              cudaStream_t st);
+
+// Step 2.  scheme 1: slices with width beta from shifts (offset 0);
+// scheme 2: symmetric residues of rint(ldexp(x, shift)).
+// Rows: A (rows x cols, row-major) -> out[s][rows_p][cols_p].
+cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift,
+                              int S, int beta, int8_t* out, size_t rows_p, size_t cols_p, int sms,
+                              cudaStream_t st);
+// Columns: B (K x N, row-major) -> out[s][Np][Kp] (transposed, K-major); also
+// writes shift[n] = offset - max exponent of column n.
+cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
+                              int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
+                              cudaStream_t st);
+
+// Step 3.
+struct GemmPlan {
+    const int8_t* a_planes;   // [planes][Mp][Kp]
+    const int8_t* b_planes;   // [planes][Np][Kp]
+    int planes;
+    size_t Mp, Np, Kp;
+    PairList pairs;
+    int32_t* ctc;             // [groups][Mp][Np]
+    int* err;                 // device error word
+    int sms;
+};
+cudaError_t launch_gemm_i8(const GemmPlan& plan, cudaStream_t st);
+
+// Step 4.
+cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S,
+                                const int32_t* shiftA, const int32_t* shiftB, double* C, cudaStream_t st);
+cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
+                                const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st);
+
+}  // namespace oza

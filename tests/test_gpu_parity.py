@@ -1,0 +1,120 @@
+"""GPU parity: every stage of the sm_100a pipeline against the CPU oracle,
+bit for bit (shifts, INT8 slices/residues, INT32 products, FP64 C), on seeded
+inputs and on the edge cases the reference's arithmetic has."""
+import numpy as np
+import pytest
+
+from tests.gpu_helpers import bits, run_pipeline
+
+pytestmark = pytest.mark.gpu
+
+
+def _oz():
+    import ozablas_b200 as oz
+    return oz
+
+
+def _check_all(got, ref):
+    assert np.array_equal(got["shift_A"], ref["shift_A"]), "shift_A"
+    assert np.array_equal(got["shift_B"], ref["shift_B"]), "shift_B"
+    assert np.array_equal(got["A_slices"], ref["A_slices"]), "A slices"
+    assert np.array_equal(got["B_slices"], ref["B_slices"]), "B slices"
+    assert np.array_equal(got["C_tc"], ref["C_tc"]), "INT32 products"
+    diff = bits(got["C"]) != bits(ref["C"])
+    assert not diff.any(), f"C differs in {int(diff.sum())} entries"
+
+
+def _padding_zero(got):
+    i = got["ws"].info
+    M, N, K = i["M"], i["N"], i["K"]
+    assert not got["A_planes"][:, M:, :].any() and not got["A_planes"][:, :, K:].any()
+    assert not got["B_planes"][:, N:, :].any() and not got["B_planes"][:, :, K:].any()
+
+
+@pytest.mark.parametrize("S", [1, 2, 4, 7, 8, 9, 12, 16, 18, 20])
+def test_scheme2_stages_bitexact(executor, S):
+    oz = _oz()
+    from oracle import Oracle
+    A = oz.generate_matrix(160, 256, 0.5, 42)
+    B = oz.generate_matrix(256, 300, 0.5, 43)
+    got = run_pipeline(oz, executor, 2, A, B, S)
+    _check_all(got, Oracle.scheme2(A, B, S))
+    _padding_zero(got)
+
+
+@pytest.mark.parametrize("S", [1, 2, 3, 5, 8, 10, 13])
+def test_scheme1_stages_bitexact(executor, S):
+    oz = _oz()
+    from oracle import Oracle
+    A = oz.generate_matrix(130, 200, 1.0, 42)
+    B = oz.generate_matrix(200, 260, 1.0, 43)
+    got = run_pipeline(oz, executor, 1, A, B, S)
+    _check_all(got, Oracle.scheme1(A, B, S))
+    _padding_zero(got)
+
+
+@pytest.mark.parametrize("scheme,S", [(2, 8), (2, 16), (1, 6)])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (7, 5, 3), (129, 257, 129), (64, 33, 1000), (300, 17, 64)])
+def test_ragged_shapes(executor, scheme, S, shape):
+    oz = _oz()
+    from oracle import Oracle
+    M, N, K = shape
+    A = oz.generate_matrix(M, K, 2.0, 11)
+    B = oz.generate_matrix(K, N, 2.0, 12)
+    got = run_pipeline(oz, executor, scheme, A, B, S)
+    ref = Oracle.scheme2(A, B, S) if scheme == 2 else Oracle.scheme1(A, B, S)
+    _check_all(got, ref)
+
+
+@pytest.mark.parametrize("scheme,S", [(2, 8), (2, 19), (1, 7)])
+def test_exponent_edge_cases(executor, scheme, S):
+    """All-zero rows/columns, exact zeros, subnormals, powers of two, values just
+    below a power of two, rows and columns scaled by 2^+-300."""
+    oz = _oz()
+    from oracle import Oracle
+    M, N, K = 96, 80, 128
+    A = oz.generate_matrix(M, K, 4.0, 5)
+    B = oz.generate_matrix(K, N, 4.0, 6)
+    rng = np.random.default_rng(1234)
+    A[rng.random(A.shape) < 0.05] = 0.0
+    B[rng.random(B.shape) < 0.05] = 0.0
+    A[3, :] = 0.0
+    B[:, 7] = 0.0
+    A[1, :] *= 2.0 ** 300
+    A[5, :] *= 2.0 ** -300
+    B[:, 17] *= 2.0 ** 300
+    B[:, 33] *= 2.0 ** -300
+    A[9, :] = np.ldexp(1.0, np.arange(K) % 9 - 4)
+    A[10, :] = np.nextafter(np.ldexp(1.0, np.arange(K) % 5), 0.0)
+    A[11, :] = 5e-324 * (np.arange(K) + 1)          # subnormals
+    B[:, 40] = -2.2250738585072014e-308 * np.arange(K)
+    got = run_pipeline(oz, executor, scheme, A, B, S)
+    ref = Oracle.scheme2(A, B, S) if scheme == 2 else Oracle.scheme1(A, B, S)
+    _check_all(got, ref)
+
+
+def test_config1_full_size_vs_oracle(executor):
+    """Config 1: 1024^3, phi = 0.5, Scheme II with 8 moduli, bit-exact end to end."""
+    oz = _oz()
+    from oracle import Oracle
+    A = oz.generate_matrix(1024, 1024, 0.5, 42)
+    B = oz.generate_matrix(1024, 1024, 0.5, 43)
+    got = run_pipeline(oz, executor, 2, A, B, 8)
+    _check_all(got, Oracle.scheme2(A, B, 8))
+
+
+def test_repeat_calls_identical(executor):
+    """Workspaces are reusable: a second call gives identical results."""
+    import torch
+    oz = _oz()
+    A = oz.generate_matrix(256, 384, 0.5, 1)
+    B = oz.generate_matrix(384, 512, 0.5, 2)
+    ws = oz.WorkspaceScheme2(executor, 256, 512, 384, 12)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    c1 = torch.empty(256, 512, dtype=torch.float64, device="cuda")
+    c2 = torch.empty_like(c1)
+    oz.ozaki_scheme2_gemm(ws, dA, dB, c1)
+    oz.ozaki_scheme2_gemm(ws, dA, dB, c2)
+    torch.cuda.synchronize()
+    assert torch.equal(c1.view(torch.int64), c2.view(torch.int64))
+    assert ws.device_error() == 0
