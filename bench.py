@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--phi", type=float, default=0.5)
     p.add_argument("--cpu-sample", type=int, default=512, help="rows/cols of the CPU block sample")
     p.add_argument("--no-extras", action="store_true", help="skip DGEMM / reference-GPU / accuracy side numbers")
+    p.add_argument("--materialize", action="store_true",
+                   help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
     return p.parse_args()
 
 
@@ -58,6 +60,7 @@ def workload(args):
     return {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{args.size}^3",
             "M": args.size, "N": args.size, "K": args.size, "scheme": args.scheme,
             "slices": args.slices, "phi": args.phi, "input_seeds": [42, 43],
+            "path": "materialized" if getattr(args, "materialize", False) else "fused",
             "layout": "row-major fp64", "l2": "inputs (1 GiB) larger than L2; no flush"}
 
 
@@ -69,6 +72,8 @@ def int8_ops(args):
 
 # ------------------------------------------------------------------ distributed
 def dist_setup(args):
+    """One process per GPU under torchrun.  NCCL where GPUs exist; gloo on a
+    CPU-only host (used by the tests of the multi-rank launch path)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -76,17 +81,22 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
     return ws, rank, local
 
 
 def dist_max(x, ws):
+    """Maximum of a per-rank float over all ranks."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -288,7 +298,8 @@ def run_ours(args, ws, rank, local):
     ex = oz.CudaExecutor(local)
     stream = torch.cuda.current_stream(dev)
     ex.set_stream(stream.cuda_stream)
-    W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, n, n, n, S)
+    W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, n, n, n, S,
+                                                                         materialize=args.materialize)
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
 

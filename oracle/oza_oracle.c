@@ -19,6 +19,7 @@
  *
  * Build: see oracle/Makefile (gcc -O2 -fopenmp -ffp-contract=off).
  */
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -220,15 +221,20 @@ void oo_slice2(const double* X, long rows, long cols, const int32_t* shifts, int
     }
 }
 
-/* double -> int8 the way sm_100 cvt.rzi does it: truncate toward zero,
- * saturate to the int8 range, NaN -> 0.  Only the NaN case is reachable for
- * finite inputs (an all-zero row in Scheme I, step2_slicing.hpp:58-66 computes
- * 0 * 2^1029 = 0 * inf); every other slice value lies in [-64, 64]. */
+/* double -> int8 the way the reference's `static_cast<int8_t>(double)`
+ * executes on the GPU (step2_slicing.hpp:66,95): a saturating conversion to
+ * int32 (truncation toward zero, NaN -> INT_MIN) whose low byte is kept.  For
+ * finite inputs the special values occur only in Scheme I rows whose maximum
+ * lies within 2^beta of the subnormal range (0 * inf = NaN -> 0, +inf -> -1,
+ * -inf -> 0); every other slice value lies in [-64, 64].  (On an x86 host the
+ * same C++ cast is undefined for these values and yields 0.) */
 static int8_t oo_cvt_s8(double v) {
-    if (v != v) return 0;
-    if (v >= 127.0) return 127;
-    if (v <= -128.0) return -128;
-    return (int8_t)(int)v;
+    int32_t i;
+    if (v != v) i = INT32_MIN;
+    else if (v >= 2147483647.0) i = INT32_MAX;
+    else if (v <= -2147483648.0) i = INT32_MIN;
+    else i = (int32_t)v;
+    return (int8_t)(uint8_t)((uint32_t)i & 0xFFu);
 }
 
 /* Scheme I slicing (step2_slicing.hpp:44-100): with e = max exponent of the

@@ -70,7 +70,9 @@ struct oza_workspace {
     unsigned long long* colmax = nullptr;
     int8_t* aplanes = nullptr;
     int8_t* bplanes = nullptr;
-    int32_t* ctc = nullptr;
+    int32_t* ctc = nullptr;          // INT32 group planes (materialised / Scheme I)
+    uint8_t* coef = nullptr;         // Scheme II CRT coefficient bytes [S][Mp][Np]
+    bool fused = false;
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     oza::PairList pairs{};
@@ -93,7 +95,7 @@ struct DeviceGuard {
 };
 
 void ws_release(oza_workspace* ws) {
-    void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->err};
+    void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->coef, ws->err};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (auto& e : ws->ev)
@@ -266,6 +268,12 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
         delete ws;
         return cuda_fail(e, "CUDA: constant table upload failed");
     }
+    // Scheme II without MATERIALIZE reduces the INT32 residue products to their
+    // one-byte CRT coefficients inside the GEMM epilogue: byte planes replace
+    // the INT32 planes (a quarter of the memory and traffic).
+    ws->fused = (scheme == OZA_SCHEME2) && !(flags & OZA_WS_MATERIALIZE);
+    const size_t ctc_bytes = ws->fused ? 0 : (size_t)ws->groups * ws->Mp * ws->Np * sizeof(int32_t) + 16;
+    const size_t coef_bytes = ws->fused ? (size_t)slices * ws->Mp * ws->Np + 16 : 0;
     struct Req {
         void** p;
         size_t bytes;
@@ -275,10 +283,12 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
         {(void**)&ws->colmax, (N ? N : 1) * sizeof(unsigned long long)},
         {(void**)&ws->aplanes, (size_t)slices * ws->Mp * ws->Kp + 16},
         {(void**)&ws->bplanes, (size_t)slices * ws->Np * ws->Kp + 16},
-        {(void**)&ws->ctc, (size_t)ws->groups * ws->Mp * ws->Np * sizeof(int32_t) + 16},
+        {(void**)&ws->ctc, ctc_bytes},
+        {(void**)&ws->coef, coef_bytes},
         {(void**)&ws->err, sizeof(int)},
     };
     for (auto& r : reqs) {
+        if (r.bytes == 0) continue;
         e = cudaMalloc(r.p, r.bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -389,19 +399,25 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         plan.Np = ws->Np;
         plan.Kp = ws->Kp;
         plan.pairs = ws->pairs;
-        plan.ctc = ws->ctc;
         plan.err = ws->err;
         plan.sms = ex->sms;
+        plan.ctc = ws->ctc;
+        plan.coef = ws->fused ? ws->coef : nullptr;
         OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[3], st), "CUDA: event record");
         // step 4
-        if (ws->scheme == OZA_SCHEME2)
+        if (ws->fused) {
+            OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef, ws->Mp, ws->Np, M, N, ws->S, ws->shiftA, ws->shiftB, C,
+                                              ex->sms, st),
+                         "step4 crt");
+        } else if (ws->scheme == OZA_SCHEME2) {
             OZA_CUDA_TRY(oza::launch_reconstruct2(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->shiftA, ws->shiftB, C, st),
                          "step4 crt");
-        else
+        } else {
             OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->beta, ws->shiftA,
                                                   ws->shiftB, C, st),
                          "step4 sum");
+        }
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[4], st), "CUDA: event record");
     }
     if (timings) {

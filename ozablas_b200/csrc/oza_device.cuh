@@ -18,7 +18,7 @@ enum DeviceError : int {
 };
 
 // Per-modulus constants for the residue and CRT arithmetic (filled on the
-// host per device, see oza_tables.cu).  For modulus m (odd, 149..251):
+// host per device by upload_tables() in oza_kernels.cu).  For modulus m (odd, 149..251):
 //   magic  = ceil(2^39 / m): floor(u / m) == umulhi(u, magic) >> 7 for u < 2^31
 //   c21/42/63 = 2^21, 2^42, 2^63 mod m, symmetric representatives
 //   inv    = (M/m)^-1 mod m for the current slice count (per table row)
@@ -36,7 +36,7 @@ struct CrtTable {
     uint32_t P[kMaxSlices][5];  // M / m_i
     uint32_t inv[kMaxSlices];   // (M / m_i)^-1 mod m_i
     uint32_t c16inv[kMaxSlices];  // (2^16 * inv_i) mod m_i
-    float recip[kMaxSlices];      // 1 / m_i (float, for the quotient estimate)
+    uint32_t recip24[kMaxSlices]; // floor(2^24 / m_i), for the quotient estimate
     int nlimbs;                   // limbs of M that can be nonzero
 };
 
@@ -61,9 +61,14 @@ __device__ __forceinline__ int frexp_exp_bits(unsigned long long mag) {
     return -1010 - __clzll((long long)mag);   // subnormal
 }
 
-// max exponent from a running maximum of magnitude bits (0 = all zero rows).
+// Max exponent from a running maximum of magnitude bits.  The reference's
+// running maximum starts at -1023 (step1_statistics.hpp:33,88), so an
+// all-zero row and a row whose largest entry is a subnormal below 2^-1024
+// (frexp exponent < -1023) both yield -1023.
 __device__ __forceinline__ int max_exp_from_bits(unsigned long long mag) {
-    return mag == 0ull ? -1023 : frexp_exp_bits(mag);
+    if (mag == 0ull) return -1023;
+    int e = frexp_exp_bits(mag);
+    return e < -1023 ? -1023 : e;
 }
 
 // ---------------------------------------------------------------------------

@@ -117,7 +117,7 @@ cudaError_t upload_tables() {
                 for (int l = 0; l < 5; ++l) t.P[i][l] = 0;
                 t.inv[i] = 0;
                 t.c16inv[i] = 0;
-                t.recip[i] = 0.f;
+                t.recip24[i] = 0;
                 continue;
             }
             Big P = big_from(1);
@@ -132,7 +132,7 @@ cudaError_t upload_tables() {
                 }
             t.inv[i] = inv;
             t.c16inv[i] = (uint32_t)((65536ull * inv) % m);
-            t.recip[i] = 1.0f / (float)m;
+            t.recip24[i] = (uint32_t)((1u << 24) / m);
         }
     }
     e = cudaMemcpyToSymbol(c_mod, mc, sizeof(mc));
@@ -306,10 +306,15 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
            ((uint32_t)(d & 0xFF) << 24);
 }
 
-// double -> int8 as the sm_100 conversion does it: truncate, saturate, NaN -> 0.
+// double -> int8 exactly as the reference's `static_cast<int8_t>(double)`
+// behaves on the GPU (step2_slicing.hpp:66,95): a saturating conversion to
+// int32 (truncation toward zero, NaN -> INT_MIN) of which the low byte is
+// kept.  In-range slice values (|v| <= 64) are unaffected; the special values
+// arise only in Scheme I rows whose maximum lies within 2^beta of the
+// subnormal range, where 2^-(e+1-beta) overflows to inf: NaN (0 * inf) -> 0,
+// +inf -> -1, -inf -> 0.
 __device__ __forceinline__ int cvt_s8(double v) {
-    int i = __double2int_rz(v);
-    return i > 127 ? 127 : (i < -128 ? -128 : i);
+    return (int)(int8_t)__double2int_rz(v);
 }
 
 // Scheme II residues of 16 consecutive values.  out16[s] receives the packed bytes.
@@ -433,31 +438,174 @@ __global__ void __launch_bounds__(256) k_slice_cols(const double* __restrict__ B
 }
 
 // ---------------------------------------------------------------------------
+// Exact CRT arithmetic (Scheme II step 4), shared by the fused GEMM epilogue
+// and the standalone reconstruction kernel
+// ---------------------------------------------------------------------------
+
+// (C * inv_s) mod m_s in [0, m_s) for any int32 C: C = hi * 2^16 + lo,
+// y = hi * ((2^16 inv) mod m) + lo * inv + m * 2^16 lies in (0, 2^31).
+__device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t magic, uint32_t inv,
+                                              uint32_t c16inv) {
+    const int hi = C >> 16;
+    const int lo = C & 0xFFFF;
+    const uint32_t u = (uint32_t)(hi * (int)c16inv + lo * (int)inv + (int)(m << 16));
+    return u - div_small(u, magic) * m;
+}
+
+// Running state of one element: T = sum c_s * (M / m_s) as NL 64-bit column
+// sums of 32-bit limb products (each below 2^45), and sum c_s * floor(2^24 / m_s)
+// for the quotient estimate.
+template <int NL>
+struct CrtAcc {
+    unsigned long long a[NL];
+    uint32_t q;
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int l = 0; l < NL; ++l) a[l] = 0ull;
+        q = 0;
+    }
+    __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) {
+#pragma unroll
+        for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)c * T.P[s][l];
+        q += c * T.recip24[s];
+    }
+};
+
+// x = T mod M, signed map at floor(M/2) (x >= floor(M/2) means -(M - x)), the
+// reference's conversion d0 + d1 2^64 + d2 2^128 over 64-bit limbs with a
+// rounding after each addition (crt_math.hpp:73-80), then ldexp(., -esum)
+// (step4_reconstruction.hpp:59-184).
+template <int NL>
+__device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>& acc, int esum) {
+    uint32_t t[NL + 1];
+    unsigned long long carry = 0;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        unsigned long long v = acc.a[l] + carry;
+        t[l] = (uint32_t)v;
+        carry = v >> 32;
+    }
+    t[NL] = (uint32_t)carry;
+    // q = floor(T / M) up to +-1: sum c_s floor(2^24/m_s) / 2^24 is within
+    // 20 * 255 / 2^24 of sum c_s / m_s = T / M.
+    const uint32_t q = acc.q >> 24;
+    uint32_t r[NL + 1];
+    long long borrow = 0;
+    unsigned long long qc = 0;
+#pragma unroll
+    for (int l = 0; l <= NL; ++l) {
+        unsigned long long qm = (unsigned long long)q * (l < NL ? T.M[l] : 0u) + qc;
+        qc = qm >> 32;
+        long long d = (long long)t[l] - (long long)(uint32_t)qm - borrow;
+        borrow = d < 0 ? 1 : 0;
+        r[l] = (uint32_t)d;
+    }
+    if (borrow) {   // q one too large: R += M
+        unsigned long long c = 0;
+#pragma unroll
+        for (int l = 0; l <= NL; ++l) {
+            unsigned long long v = (unsigned long long)r[l] + (l < NL ? T.M[l] : 0u) + c;
+            r[l] = (uint32_t)v;
+            c = v >> 32;
+        }
+    } else {        // q one too small: R >= M, R -= M
+        bool ge = true;
+        if (r[NL] == 0) {
+#pragma unroll
+            for (int l = NL - 1; l >= 0; --l) {
+                if (r[l] != T.M[l]) {
+                    ge = r[l] > T.M[l];
+                    break;
+                }
+            }
+        }
+        if (ge) {
+            long long b = 0;
+#pragma unroll
+            for (int l = 0; l <= NL; ++l) {
+                long long d = (long long)r[l] - (long long)(l < NL ? T.M[l] : 0u) - b;
+                b = d < 0 ? 1 : 0;
+                r[l] = (uint32_t)d;
+            }
+        }
+    }
+    bool neg = true;
+#pragma unroll
+    for (int l = NL - 1; l >= 0; --l) {
+        if (r[l] != T.Mhalf[l]) {
+            neg = r[l] > T.Mhalf[l];
+            break;
+        }
+    }
+    if (neg) {
+        long long b = 0;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            long long d = (long long)T.M[l] - (long long)r[l] - b;
+            b = d < 0 ? 1 : 0;
+            r[l] = (uint32_t)d;
+        }
+    }
+    double mag = __ull2double_rn((unsigned long long)r[0] | (NL > 1 ? (unsigned long long)r[1] << 32 : 0ull));
+    if (NL > 2) {
+        unsigned long long w1 = (unsigned long long)r[2] | (NL > 3 ? (unsigned long long)r[3] << 32 : 0ull);
+        mag = __dadd_rn(mag, __ull2double_rn(w1) * 0x1p64);
+    }
+    if (NL > 4) mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)r[4]) * 0x1p128);
+    return ldexp(neg ? -mag : mag, -esum);
+}
+
+// ---------------------------------------------------------------------------
 // Step 3: tcgen05 INT8 GEMM
 // ---------------------------------------------------------------------------
-constexpr int kGemmThreads = 192;   // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+// One persistent CTA per SM walks output tiles (128 x 256); for each tile it
+// runs every group g (Scheme II: residue g, A_g * B_g^T; Scheme I: the slice
+// pairs with s + t = g + 2) into one of two TMEM accumulators, so the
+// epilogue of unit (tile, g) overlaps the MMAs of unit (tile, g + 1).
+//   warp 0      TMA producer (4-stage ring of A 128x128 + B^T 256x128 int8 tiles)
+//   warp 1      TMEM allocation, UMMA issue (one elected lane)
+//   warps 2..9  epilogue; warp w reads TMEM lanes 32 (w % 4).. and column half (w - 2) / 4
+// Epilogues: kEpiI32 writes the INT32 group planes; kEpiCoef (Scheme II)
+// reduces each residue product to its one-byte CRT coefficient and writes the
+// byte planes, which k_crt_coef turns into FP64 C (a quarter of the INT32
+// traffic, and the multiword CRT runs at full occupancy instead of in the 8
+// epilogue warps, where it would stall the MMA pipeline).
+constexpr int kEpiWarps = 8;
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;
 constexpr int kStages = 4;
 constexpr int kABytes = kTileM * kTileK;   // 16 KB per stage
 constexpr int kBBytes = kTileN * kTileK;   // 32 KB per stage
 constexpr uint32_t kAccCols = kTileN;      // TMEM columns per accumulator
 constexpr uint32_t kTmemCols = 2 * kAccCols;
 constexpr int kGemmSmem = kStages * (kABytes + kBBytes) + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int kEpiI32 = 0;
+constexpr int kEpiCoef = 1;
 
 struct GemmArgs {
-    int m_tiles, n_tiles, k_blocks, total_tiles;
+    int m_tiles, n_tiles, k_blocks, total_tiles, groups;
+    int band;                     // m-tiles per rasterisation band
     long long Mp, Np;
-    int32_t* ctc;
     int* err;
+    int32_t* ctc;                 // kEpiI32: [groups][Mp][Np]
+    uint8_t* coef;                // kEpiCoef: [S][Mp][Np] CRT coefficient bytes
+    int S;
 };
 
-__device__ __forceinline__ void decode_tile(int t, const GemmArgs& g, int& grp, int& mt, int& nt) {
-    const int per = g.m_tiles * g.n_tiles;
-    grp = t / per;
-    const int rem = t - grp * per;
-    mt = rem / g.n_tiles;
-    nt = rem - mt * g.n_tiles;
+// Tile t -> (mt, nt).  Tiles are walked in bands of `band` m-tiles, n-major
+// inside a band, so the ~148 tiles in flight at once cover a band x (148/band)
+// block: per residue plane they touch band * 1 MB of A and 148/band * 2 MB of
+// B^T (at K = 8192), which stays L2-resident while every CTA cycles through
+// the S planes of its own tile.
+__device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, int& nt) {
+    const int per_band = a.band * a.n_tiles;
+    const int b = t / per_band;
+    const int tb = t - b * per_band;
+    const int rows = min(a.band, a.m_tiles - b * a.band);
+    nt = tb / rows;
+    mt = b * a.band + (tb - nt * rows);
 }
 
+template <int EPI>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const __grid_constant__ PairList pairs, const GemmArgs args) {
@@ -474,6 +622,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = args.groups;
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
             mbar_init(&full[i], 1);
@@ -481,8 +630,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         }
         mbar_init(&acc_full[0], 1);
         mbar_init(&acc_full[1], 1);
-        mbar_init(&acc_empty[0], 4);
-        mbar_init(&acc_empty[1], 4);
+        mbar_init(&acc_empty[0], kEpiWarps);
+        mbar_init(&acc_empty[1], kEpiWarps);
         mbar_init(drain, 1);
         *abort_flag = 0;
         fence_barrier_init();
@@ -505,26 +654,28 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         long long issued = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
-            int grp, mt, nt;
-            decode_tile(t, args, grp, mt, nt);
-            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kTileM);
-                const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN);
-                for (int kb = 0; kb < args.k_blocks; ++kb) {
-                    int w = 1;
-                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
-                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                    if (!ok) break;
-                    if (lane == 0) {
-                        mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
-                        tma_load_2d(sA + stage * kABytes, &tmA, &full[stage], kb * kTileK, arow);
-                        tma_load_2d(sB + stage * kBBytes, &tmB, &full[stage], kb * kTileK, brow);
-                    }
-                    __syncwarp();
-                    ++issued;
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
+            int mt, nt;
+            tile_coords(t, args, mt, nt);
+            for (int grp = 0; grp < G && ok; ++grp) {
+                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                    const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kTileM);
+                    const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN);
+                    for (int kb = 0; kb < args.k_blocks; ++kb) {
+                        int w = 1;
+                        if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
+                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                        if (!ok) break;
+                        if (lane == 0) {
+                            mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
+                            tma_load_2d(sA + stage * kABytes, &tmA, &full[stage], kb * kTileK, arow);
+                            tma_load_2d(sB + stage * kBBytes, &tmB, &full[stage], kb * kTileK, brow);
+                        }
+                        __syncwarp();
+                        ++issued;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
             }
@@ -545,47 +696,47 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint32_t phase = 0;
         int local = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x, ++local) {
-            int grp, mt, nt;
-            decode_tile(t, args, grp, mt, nt);
-            const int acc = local & 1;
-            const uint32_t acc_phase = (local >> 1) & 1;
-            int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
-            ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-            if (!ok) break;
-            tc_fence_after();
-            const uint32_t d = tmem_base + acc * kAccCols;
-            uint32_t accumulate = 0;
-            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                for (int kb = 0; kb < args.k_blocks; ++kb) {
-                    w = 1;
-                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
-                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                    if (!ok) break;
-                    tc_fence_after();
-                    if (lane == 0) {
-                        const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
-                        const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
+        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+            for (int grp = 0; grp < G && ok; ++grp, ++local) {
+                const int acc = local & 1;
+                const uint32_t acc_phase = (local >> 1) & 1;
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
+                ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + acc * kAccCols;
+                uint32_t accumulate = 0;
+                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                    for (int kb = 0; kb < args.k_blocks; ++kb) {
+                        w = 1;
+                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
+                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                        if (!ok) break;
+                        tc_fence_after();
+                        if (lane == 0) {
+                            const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
+                            const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
 #pragma unroll
-                        for (int k = 0; k < kTileK / 32; ++k) {
-                            // +32 bytes of K inside the swizzle row = +2 in 16-byte units
-                            umma_i8(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
-                            accumulate = 1;
+                            for (int k = 0; k < kTileK / 32; ++k) {
+                                // +32 bytes of K inside the swizzle row = +2 in 16-byte units
+                                umma_i8(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
+                                accumulate = 1;
+                            }
+                            umma_commit(&empty[stage]);
                         }
-                        umma_commit(&empty[stage]);
-                    }
-                    __syncwarp();
-                    accumulate = 1;
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
+                        __syncwarp();
+                        accumulate = 1;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
+                if (!ok) break;
+                if (lane == 0) umma_commit(&acc_full[acc]);
+                __syncwarp();
             }
-            if (!ok) break;
-            if (lane == 0) umma_commit(&acc_full[acc]);
-            __syncwarp();
         }
         if (!ok && lane == 0) {
             // Wait for the MMAs already issued before TMEM is released.
@@ -594,34 +745,72 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             mbar_wait(drain, 0, &no_abort, nullptr);
         }
     } else {
-        // ---------------- epilogue: TMEM -> INT32 planes ----------------
-        const int q = warp & 3;   // TMEM lane quadrant this warp may access
+        // ---------------- epilogue ----------------
+        const int q = warp & 3;                 // TMEM lane quadrant this warp may access
+        const int half = (warp - 2) >> 2;       // column half of the tile
+        const int row_local = q * 32 + lane;
         int local = 0;
-        for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x, ++local) {
-            int grp, mt, nt;
-            decode_tile(t, args, grp, mt, nt);
-            const int acc = local & 1;
-            const uint32_t acc_phase = (local >> 1) & 1;
-            int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
-            if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) break;
-            tc_fence_after();
-            const long long row = (long long)mt * kTileM + q * 32 + lane;
-            int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np + (size_t)nt * kTileN;
-            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols;
+        bool ok = true;
+        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+            int mt, nt;
+            tile_coords(t, args, mt, nt);
+            const long long row = (long long)mt * kTileM + row_local;
+            for (int grp = 0; grp < G; ++grp, ++local) {
+                const int acc = local & 1;
+                const uint32_t acc_phase = (local >> 1) & 1;
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
+                if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t taddr =
+                    tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
+                if (EPI == kEpiI32) {
+                    int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+                                   (size_t)nt * kTileN + half * (kTileN / 2);
 #pragma unroll 1
-            for (int c = 0; c < kTileN / 32; ++c) {
-                uint32_t r[32];
-                tmem_ld32(taddr + c * 32, r);
-                tmem_ld_wait();
-                int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+                    for (int c = 0; c < kTileN / 64; ++c) {
+                        uint32_t r[32];
+                        tmem_ld32(taddr + c * 32, r);
+                        tmem_ld_wait();
+                        int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
 #pragma unroll
-                for (int v = 0; v < 8; ++v)
-                    d4[v] = make_int4((int)r[4 * v], (int)r[4 * v + 1], (int)r[4 * v + 2], (int)r[4 * v + 3]);
+                        for (int v = 0; v < 8; ++v)
+                            d4[v] = make_int4((int)r[4 * v], (int)r[4 * v + 1], (int)r[4 * v + 2], (int)r[4 * v + 3]);
+                    }
+                } else {
+                    // Scheme II: reduce each INT32 residue product to its CRT
+                    // coefficient ((C mod m_g) * inv_g) mod m_g, one byte.
+                    const ModConst mc = c_mod[grp];
+                    const uint32_t inv = c_crt[args.S - 1].inv[grp], c16 = c_crt[args.S - 1].c16inv[grp];
+                    uint8_t* dst = args.coef + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+                                   (size_t)nt * kTileN + half * (kTileN / 2);
+#pragma unroll 1
+                    for (int c = 0; c < kTileN / 64; ++c) {
+                        uint32_t r[32];
+                        tmem_ld32(taddr + c * 32, r);
+                        tmem_ld_wait();
+                        uint32_t wds[8];
+#pragma unroll
+                        for (int v = 0; v < 8; ++v) {
+                            uint32_t b0 = crt_coeff((int32_t)r[4 * v], mc.m, mc.magic, inv, c16);
+                            uint32_t b1 = crt_coeff((int32_t)r[4 * v + 1], mc.m, mc.magic, inv, c16);
+                            uint32_t b2 = crt_coeff((int32_t)r[4 * v + 2], mc.m, mc.magic, inv, c16);
+                            uint32_t b3 = crt_coeff((int32_t)r[4 * v + 3], mc.m, mc.magic, inv, c16);
+                            wds[v] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+                        }
+                        uint4* d4 = reinterpret_cast<uint4*>(dst + c * 32);
+                        d4[0] = make_uint4(wds[0], wds[1], wds[2], wds[3]);
+                        d4[1] = make_uint4(wds[4], wds[5], wds[6], wds[7]);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[acc]);
+
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[acc]);
         }
     }
 
@@ -637,122 +826,38 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 // Step 4: reconstruction
 // ---------------------------------------------------------------------------
 
-// (C * inv_s) mod m_s in [0, m_s) for any int32 C: C = hi * 2^16 + lo,
-// y = hi * ((2^16 inv) mod m) + lo * inv + m * 2^16 lies in (0, 2^31).
-__device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t magic, uint32_t inv,
-                                              uint32_t c16inv) {
-    const int hi = C >> 16;
-    const int lo = C & 0xFFFF;
-    const uint32_t u = (uint32_t)(hi * (int)c16inv + lo * (int)inv + (int)(m << 16));
-    return u - div_small(u, magic) * m;
-}
-
-// Exact CRT reconstruction of one element from its S INT32 products, then the
-// reference's conversion (step4_reconstruction.hpp:59-184, crt_math.hpp:73-80):
-// T = sum c_s * (M/m_s); x = T mod M; if x >= floor(M/2) the value is -(M-x);
-// magnitude to double as d0 + d1 2^64 + d2 2^128 (64-bit limbs, rounding after
-// each add); finally ldexp(., -(shift_A + shift_B)).
+// Scheme II step 4 from the coefficient byte planes [S][Mp][Np] written by the
+// GEMM epilogue: one thread per 4 consecutive columns of a row (a warp reads
+// 128 contiguous bytes per plane), exact CRT per element, FP64 C.  Few
+// registers per thread, so the multiword arithmetic runs at full occupancy.
 template <int NL>
-__device__ __forceinline__ double crt_to_double(const int32_t* vals, int S, int esum) {
+__global__ void __launch_bounds__(256) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
+                                                  long long M, long long N, int S, const int32_t* __restrict__ sA,
+                                                  const int32_t* __restrict__ sB, double* __restrict__ C) {
+    const long long chunks = (N + 3) >> 2;
+    const long long total = M * chunks;
+    const size_t plane = (size_t)Mp * (size_t)Np;
     const CrtTable& T = c_crt[S - 1];
-    unsigned long long acc[NL];
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const long long i = id / chunks, j0 = (id - i * chunks) << 2;
+        const uint8_t* src = coef + (size_t)i * Np + j0;
+        CrtAcc<NL> st[4];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) acc[l] = 0ull;
-    float qf = 0.f;
-    for (int s = 0; s < S; ++s) {
-        const uint32_t m = c_mod[s].m;
-        const uint32_t c = crt_coeff(vals[s], m, c_mod[s].magic, T.inv[s], T.c16inv[s]);
+        for (int e = 0; e < 4; ++e) st[e].zero();
+        for (int s = 0; s < S; ++s) {
+            const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)s * plane));
 #pragma unroll
-        for (int l = 0; l < NL; ++l) acc[l] += (unsigned long long)c * T.P[s][l];
-        qf = fmaf((float)c, T.recip[s], qf);
-    }
-    // carry-normalise T into NL+1 32-bit limbs
-    uint32_t t[NL + 1];
-    unsigned long long carry = 0;
+            for (int e = 0; e < 4; ++e) st[e].add(T, s, (w >> (e * 8)) & 0xFFu);
+        }
+        const int sa = sA[i];
+        double* crow = C + i * N;
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        unsigned long long v = acc[l] + carry;
-        t[l] = (uint32_t)v;
-        carry = v >> 32;
-    }
-    t[NL] = (uint32_t)carry;
-    // R = T - q M with q = floor(T / M) estimated in float (|error| < 1), then one fix-up.
-    const uint32_t q = (uint32_t)floorf(qf);
-    long long borrow = 0;
-    uint32_t r[NL + 1];
-    {
-        unsigned long long qc = 0;
-#pragma unroll
-        for (int l = 0; l <= NL; ++l) {
-            unsigned long long qm = (unsigned long long)q * (l < NL ? T.M[l] : 0u) + qc;
-            qc = qm >> 32;
-            long long d = (long long)t[l] - (long long)(uint32_t)qm - borrow;
-            borrow = d < 0 ? 1 : 0;
-            r[l] = (uint32_t)d;
+        for (int e = 0; e < 4; ++e) {
+            const long long j = j0 + e;
+            if (j < N) crow[j] = crt_finish<NL>(T, st[e], sa + sB[j]);
         }
     }
-    if (borrow) {   // estimate one too large: R += M
-        unsigned long long c = 0;
-#pragma unroll
-        for (int l = 0; l <= NL; ++l) {
-            unsigned long long v = (unsigned long long)r[l] + (l < NL ? T.M[l] : 0u) + c;
-            r[l] = (uint32_t)v;
-            c = v >> 32;
-        }
-    } else {
-        // R >= M ?  then R -= M
-        bool ge = true;
-        if (r[NL] != 0) {
-            ge = true;
-        } else {
-#pragma unroll
-            for (int l = NL - 1; l >= 0; --l) {
-                if (r[l] != T.M[l]) {
-                    ge = r[l] > T.M[l];
-                    break;
-                }
-            }
-        }
-        if (ge) {
-            long long b = 0;
-#pragma unroll
-            for (int l = 0; l <= NL; ++l) {
-                long long d = (long long)r[l] - (long long)(l < NL ? T.M[l] : 0u) - b;
-                b = d < 0 ? 1 : 0;
-                r[l] = (uint32_t)d;
-            }
-        }
-    }
-    // signed map at floor(M/2)
-    bool neg = true;
-#pragma unroll
-    for (int l = NL - 1; l >= 0; --l) {
-        if (r[l] != T.Mhalf[l]) {
-            neg = r[l] > T.Mhalf[l];
-            break;
-        }
-    }
-    if (neg) {
-        long long b = 0;
-#pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            long long d = (long long)T.M[l] - (long long)r[l] - b;
-            b = d < 0 ? 1 : 0;
-            r[l] = (uint32_t)d;
-        }
-    }
-    // 4-limb (64-bit) sum as the reference converts it
-    double mag = 0.0;
-    mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)r[0] | (NL > 1 ? (unsigned long long)r[1] << 32 : 0ull)));
-    if (NL > 2) {
-        unsigned long long w1 = (unsigned long long)r[2] | (NL > 3 ? (unsigned long long)r[3] << 32 : 0ull);
-        mag = __dadd_rn(mag, __ull2double_rn(w1) * 0x1p64);
-    }
-    if (NL > 4) {
-        unsigned long long w2 = (unsigned long long)r[4];
-        mag = __dadd_rn(mag, __ull2double_rn(w2) * 0x1p128);
-    }
-    return ldexp(neg ? -mag : mag, -esum);
 }
 
 template <int NL>
@@ -762,15 +867,19 @@ __global__ void __launch_bounds__(256) k_reconstruct2(const int32_t* __restrict_
                                                       const int32_t* __restrict__ sB, double* __restrict__ C) {
     const long long total = M * N;
     const size_t plane = (size_t)Mp * (size_t)Np;
+    const CrtTable& T = c_crt[S - 1];
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
          id += (long long)gridDim.x * blockDim.x) {
         const long long i = id / N, j = id - i * N;
-        int32_t vals[kMaxSlices];
         const int32_t* src = ctc + (size_t)i * Np + j;
-#pragma unroll
-        for (int s = 0; s < kMaxSlices; ++s)
-            if (s < S) vals[s] = __ldg(src + (size_t)s * plane);
-        C[id] = crt_to_double<NL>(vals, S, sA[i] + sB[j]);
+        CrtAcc<NL> st;
+        st.zero();
+        for (int s = 0; s < S; ++s) {
+            const uint32_t c = crt_coeff(__ldg(src + (size_t)s * plane), c_mod[s].m, c_mod[s].magic, T.inv[s],
+                                         T.c16inv[s]);
+            st.add(T, s, c);
+        }
+        C[id] = crt_finish<NL>(T, st, sA[i] + sB[j]);
     }
 }
 
@@ -901,29 +1010,40 @@ cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+template <int EPI>
+static cudaError_t gemm_launch(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
+                               const GemmArgs& a, int grid, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_gemm_i8<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
     });
-    if (attr_err != cudaSuccess) return attr_err;
+    if (attr != cudaSuccess) return attr;
+    k_gemm_i8<EPI><<<grid, kGemmThreads, kGemmSmem, st>>>(tmA, tmB, pairs, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     CUtensorMap tmA, tmB;
     if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, kTileM)) return cudaErrorInvalidValue;
     if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, kTileN)) return cudaErrorInvalidValue;
-    GemmArgs a;
+    GemmArgs a{};
     a.m_tiles = (int)(p.Mp / kTileM);
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
-    a.total_tiles = a.m_tiles * a.n_tiles * p.pairs.num_groups;
+    a.total_tiles = a.m_tiles * a.n_tiles;
+    a.band = a.m_tiles < 16 ? a.m_tiles : 16;
+    a.groups = p.pairs.num_groups;
     a.Mp = (long long)p.Mp;
     a.Np = (long long)p.Np;
-    a.ctc = p.ctc;
     a.err = p.err;
-    if (a.total_tiles == 0) return cudaSuccess;
-    int grid = a.total_tiles < p.sms ? a.total_tiles : p.sms;
-    k_gemm_i8<<<grid, kGemmThreads, kGemmSmem, st>>>(tmA, tmB, p.pairs, a);
-    return cudaGetLastError();
+    a.ctc = p.ctc;
+    a.coef = p.coef;
+    a.S = p.planes;
+    if (a.total_tiles == 0 || a.groups == 0) return cudaSuccess;
+    const int grid = a.total_tiles < p.sms ? a.total_tiles : p.sms;
+    return p.coef ? gemm_launch<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
+                  : gemm_launch<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);
 }
 
 cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S,
@@ -942,6 +1062,21 @@ cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t
         case 3: k_reconstruct2<3><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
         case 4: k_reconstruct2<4><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
         default: k_reconstruct2<5><<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M, size_t N, int S,
+                            const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st) {
+    long long total = (long long)M * (long long)((N + 3) / 4);
+    if (total == 0) return cudaSuccess;
+    int grid = grid_for(total, 256, sms, 16);
+    switch ((S + 3) / 4) {   // 32-bit limbs of M
+        case 1: k_crt_coef<1><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 2: k_crt_coef<2><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 3: k_crt_coef<3><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        case 4: k_crt_coef<4><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+        default: k_crt_coef<5><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
     }
     return cudaGetLastError();
 }

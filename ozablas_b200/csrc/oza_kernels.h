@@ -57,15 +57,20 @@ struct GemmPlan {
     int planes;
     size_t Mp, Np, Kp;
     PairList pairs;
-    int32_t* ctc;             // [groups][Mp][Np]
     int* err;                 // device error word
     int sms;
+    // epilogue output: INT32 group planes, or (Scheme II) CRT coefficient bytes
+    int32_t* ctc;             // [groups][Mp][Np], used when coef == nullptr
+    uint8_t* coef;            // [S][Mp][Np]
 };
 cudaError_t launch_gemm_i8(const GemmPlan& plan, cudaStream_t st);
 
 // Step 4.
 cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S,
                                 const int32_t* shiftA, const int32_t* shiftB, double* C, cudaStream_t st);
+// Scheme II step 4 from the GEMM's coefficient byte planes.
+cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M, size_t N, int S,
+                            const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st);
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
                                 const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st);
 

@@ -18,8 +18,7 @@ def run_pipeline(oz, executor, scheme, A, B, S, materialize=True):
     t = oz.OzaTimings()
     fn(ws, dA, dB, dC, t)
     out = dict(C=dC.cpu().numpy(), timings=t, ws=ws)
-    if materialize:
-        out.update(read_intermediates(executor, ws))
+    out.update(read_intermediates(executor, ws))
     return out
 
 
@@ -38,9 +37,12 @@ def read_intermediates(executor, ws):
     sB = _read(executor, ws.get_shift_B(), (N,), np.int32)
     Ap = _read(executor, ws.get_A_slices(), (S, Mp, Kp), np.int8)
     Bp = _read(executor, ws.get_B_slices(), (S, Np, Kp), np.int8)
-    Cp = _read(executor, ws.get_C_tc(), (G, Mp, Np), np.int32)
-    return dict(shift_A=sA, shift_B=sB, A_slices=Ap[:, :M, :K], B_slices=Bp[:, :N, :K].transpose(0, 2, 1),
-                C_tc=Cp[:, :M, :N], A_planes=Ap, B_planes=Bp, C_planes=Cp)
+    out = dict(shift_A=sA, shift_B=sB, A_slices=Ap[:, :M, :K], B_slices=Bp[:, :N, :K].transpose(0, 2, 1),
+               A_planes=Ap, B_planes=Bp)
+    if ws.get_C_tc():   # absent when Scheme II runs the CRT inside the GEMM epilogue
+        Cp = _read(executor, ws.get_C_tc(), (G, Mp, Np), np.int32)
+        out.update(C_tc=Cp[:, :M, :N], C_planes=Cp)
+    return out
 
 
 def bits(x):

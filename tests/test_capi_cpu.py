@@ -1,0 +1,108 @@
+"""The C-ABI library on a host without a GPU: it loads, exports every symbol
+include/oza_capi.h declares and the drop-in C++ API, its host utilities match
+the reference, and its argument checks fail cleanly.  No GPU compute."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import ozablas_b200 as oz
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_library_exports_every_declared_symbol():
+    L = oz.lib()
+    declared = oz.exported_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", oz.LIB_PATH], capture_output=True, text=True).stdout
+    for name in declared:
+        assert f" T {name}\n" in out, name
+
+
+def test_library_exports_drop_in_cxx_api():
+    out = subprocess.run(["nm", "-DC", "--defined-only", oz.LIB_PATH], capture_output=True, text=True).stdout
+    for sym in ("ozablas::ozaki_scheme1_gemm(ozablas::WorkspaceScheme1&, double const*, double const*, double*, "
+                "ozablas::OzaTimings*)",
+                "ozablas::ozaki_scheme2_gemm(ozablas::WorkspaceScheme2&, double const*, double const*, double*, "
+                "ozablas::OzaTimings*)",
+                "ozablas::CudaExecutor::CudaExecutor(int)",
+                "ozablas::WorkspaceScheme2::WorkspaceScheme2(std::shared_ptr<ozablas::Executor const>, unsigned long, "
+                "unsigned long, unsigned long, int)",
+                "ozablas::WorkspaceScheme1::get_C_tc() const"):
+        assert sym in out, sym
+
+
+def test_library_has_no_cpu_fallback_symbols():
+    """The product library links nothing from the oracle."""
+    out = subprocess.run(["nm", "-D", oz.LIB_PATH], capture_output=True, text=True).stdout
+    assert " oo_" not in out and " ref_" not in out
+
+
+def test_version_and_errors():
+    L = oz.lib()
+    assert b"sm_100a" in L.oza_version()
+    h = ctypes.c_void_p()
+    assert L.oza_ws_create(None, 2, 8, 8, 8, 8, 0, ctypes.byref(h)) == oz.OZA_INVALID_ARG
+    assert b"Executor cannot be null" in L.oza_last_error_string()
+    assert L.oza_gemm(None, None, None, None, None) == oz.OZA_INVALID_ARG
+    assert L.oza_ws_get_ptr(None, 0, ctypes.byref(h)) == oz.OZA_INVALID_ARG
+
+
+def test_executor_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(oz.OzaError):
+        oz.CudaExecutor(0)
+
+
+def test_python_api_argument_checks():
+    with pytest.raises(ValueError):
+        oz.WorkspaceScheme2(None, 4, 4, 4, 8)
+    with pytest.raises(oz.OzaError):
+        oz.WorkspaceScheme2(oz.CpuExecutor(), 4, 4, 4, 8)
+
+
+def test_generator_matches_reference_fixture():
+    g = np.load(os.path.join(GOLDEN, "generator.npz"))
+    for i in range(4):
+        r, c, phi, seed = g[f"params{i}"]
+        got = oz.generate_matrix(int(r), int(c), float(phi), int(seed))
+        assert np.array_equal(got.view(np.int64), g[f"case{i}"].view(np.int64))
+
+
+@pytest.mark.parametrize("K", [1, 5, 64, 1000, 1024, 8192, 65536, 100000])
+def test_host_scheme_parameters_match_oracle(K):
+    from oracle import Oracle
+    assert oz.scheme1_beta(K) == Oracle.beta(K)
+    for S in range(1, 21):
+        assert oz.scheme2_k_param(S, K) == Oracle.k_param(S, K)
+
+
+def test_headers_compile_standalone(tmp_path):
+    """The drop-in headers compile and link against the library (no GPU needed)."""
+    src = tmp_path / "use.cpp"
+    src.write_text(r'''
+#include <ozablas/ozablas.hpp>
+#include <ozablas/core/executor.hpp>
+#include <ozablas/core/workspace.hpp>
+#include <oza_capi.h>
+#include <cstdio>
+int main() {
+    ozablas::OzaTimings t;
+    std::printf("%s %f\n", oza_version(), t.total_ms);
+    try { ozablas::HipExecutor h(0); } catch (const std::runtime_error&) { std::printf("hip rejected\n"); }
+    return 0;
+}
+''')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "use"
+    subprocess.run(["/usr/bin/g++", "-std=c++17", f"-I{root}/include", str(src), "-o", str(exe),
+                    f"-L{root}/ozablas_b200", "-loza_b200", f"-Wl,-rpath,{root}/ozablas_b200"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "sm_100a" in out and "hip rejected" in out
