@@ -383,7 +383,7 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, st), "step1 cols");
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[1], st), "CUDA: event record");
         // step 2
-        OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A, M, K, ws->shiftA, ws->S, ws->beta, ws->aplanes, ws->Mp,
+        OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A, M, K, ws->shiftA, ws->S, ws->beta, offset, ws->aplanes, ws->Mp,
                                             ws->Kp, ex->sms, st),
                      "step2 rows");
         OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,

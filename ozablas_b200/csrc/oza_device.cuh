@@ -37,6 +37,9 @@ struct CrtTable {
     uint32_t inv[kMaxSlices];   // (M / m_i)^-1 mod m_i
     uint32_t c16inv[kMaxSlices];  // (2^16 * inv_i) mod m_i
     uint32_t recip24[kMaxSlices]; // floor(2^24 / m_i), for the quotient estimate
+    // Residue pairs (2p, 2p+1): c_a M/m_a + c_b M/m_b = (c_a m_b + c_b m_a) M/(m_a m_b)
+    uint32_t PP[kMaxSlices / 2][5];      // M / (m_2p m_2p+1)
+    uint32_t precip24[kMaxSlices / 2];   // floor(2^24 / (m_2p m_2p+1))
     int nlimbs;                   // limbs of M that can be nonzero
 };
 

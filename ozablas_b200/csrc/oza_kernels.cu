@@ -134,6 +134,17 @@ cudaError_t upload_tables() {
             t.c16inv[i] = (uint32_t)((65536ull * inv) % m);
             t.recip24[i] = (uint32_t)((1u << 24) / m);
         }
+        for (int p = 0; p < kMaxSlices / 2; ++p) {
+            const int a = 2 * p, b = 2 * p + 1;
+            for (int l = 0; l < 5; ++l) t.PP[p][l] = 0;
+            t.precip24[p] = 0;
+            if (b >= S) continue;
+            Big P = big_from(1);
+            for (int j = 0; j < S; ++j)
+                if (j != a && j != b) P = big_mul_small(P, kModuli[j]);
+            for (int l = 0; l < 5; ++l) t.PP[p][l] = P.w[l];
+            t.precip24[p] = (uint32_t)((1u << 24) / (kModuli[a] * kModuli[b]));
+        }
     }
     e = cudaMemcpyToSymbol(c_mod, mc, sizeof(mc));
     if (e != cudaSuccess) return e;
@@ -267,21 +278,28 @@ __device__ __forceinline__ double pow2_or_zero(int sh) {
     return (sh >= -1022 && sh <= 1023) ? __longlong_as_double((long long)(sh + 1023) << 52) : 0.0;
 }
 
-// Radix-2^21 split of an integer-valued double |x| < 2^84 into int32 digits.
-template <bool FOUR>
+// Radix-2^21 digits of the integer-valued double x.  NARROW (|x| <= 2^62, which
+// holds whenever K_param <= 62, i.e. always for S <= 16): one conversion to
+// int64 and two's-complement digit fields d0, d1 in [0, 2^21), d2 signed.
+// WIDE (|x| < 2^84): signed digits peeled off in double precision.
+template <bool WIDE>
 __device__ __forceinline__ void split21(double x, int& d0, int& d1, int& d2, int& d3) {
-    double r = x;
-    if (FOUR) {
-        double q3 = rint(r * 0x1p-63);
-        r = r - q3 * 0x1p63;
-        d3 = __double2int_rn(q3);
-    } else {
+    if (!WIDE) {
+        const long long t = __double2ll_rn(x);
+        d0 = (int)(t & 0x1FFFFF);
+        d1 = (int)((t >> 21) & 0x1FFFFF);
+        d2 = (int)(t >> 42);
         d3 = 0;
+        return;
     }
-    double q2 = rint(r * 0x1p-42);
+    double r = x;
+    const double q3 = rint(r * 0x1p-63);
+    r = r - q3 * 0x1p63;
+    const double q2 = rint(r * 0x1p-42);
     r = r - q2 * 0x1p42;
-    double q1 = rint(r * 0x1p-21);
+    const double q1 = rint(r * 0x1p-21);
     r = r - q1 * 0x1p21;
+    d3 = __double2int_rn(q3);
     d2 = __double2int_rn(q2);
     d1 = __double2int_rn(q1);
     d0 = __double2int_rn(r);
@@ -290,14 +308,15 @@ __device__ __forceinline__ void split21(double x, int& d0, int& d1, int& d2, int
 // Symmetric residue in [-(m-1)/2, (m-1)/2] of the integer with digits d (radix
 // 2^21), modulo c_mod[s].m.  y = sum d_i * (2^(21 i) mod m) stays below 2^29
 // in magnitude, the bias m * 2^22 makes it positive and below 2^31, and the
-// magic-number division is exact there.
-template <bool FOUR>
+// magic-number division is exact there.  With s known at compile time the
+// constants are instruction operands.
+template <bool WIDE>
 __device__ __forceinline__ int symmetric_residue(int s, int d0, int d1, int d2, int d3) {
-    const ModConst mc = c_mod[s];
+    const ModConst& mc = c_mod[s];
     int y = d0 + d1 * mc.c21 + d2 * mc.c42;
-    if (FOUR) y += d3 * mc.c63;
-    uint32_t u = (uint32_t)(y + (int)(mc.m << 22));
-    uint32_t r = u - div_small(u, mc.magic) * mc.m;
+    if (WIDE) y += d3 * mc.c63;
+    const uint32_t u = (uint32_t)(y + (int)(mc.m << 22));
+    const uint32_t r = u - div_small(u, mc.magic) * mc.m;
     return (int)r - ((r > (mc.m >> 1)) ? (int)mc.m : 0);
 }
 
@@ -317,26 +336,30 @@ __device__ __forceinline__ int cvt_s8(double v) {
     return (int)(int8_t)__double2int_rz(v);
 }
 
-// Scheme II residues of 16 consecutive values.  out16[s] receives the packed bytes.
-template <bool FOUR>
-__device__ __forceinline__ void residues16(const double (&v)[16], int sh, double p, int S, uint4* dst,
-                                           size_t plane_stride) {
-    int d0[16], d1[16], d2[16], d3[16];
+// Scheme II residues of E (8 or 16) consecutive values: plane s of dst receives
+// the E packed residues modulo m_s (reference slice_scheme2_A/B,
+// step2_slicing.hpp:110-206: x = rint(ldexp(v, shift)), symmetric residues).
+template <int S, bool WIDE, int E>
+__device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p, int8_t* dst, size_t plane_stride) {
+    int d0[E], d1[E], d2[E], d3[E];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        double x = rint(scale_pow2(v[i], sh, p));
-        split21<FOUR>(x, d0[i], d1[i], d2[i], d3[i]);
+    for (int i = 0; i < E; ++i) {
+        const double x = rint(scale_pow2(v[i], sh, p));
+        split21<WIDE>(x, d0[i], d1[i], d2[i], d3[i]);
     }
-    for (int s = 0; s < S; ++s) {
-        int r[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) r[i] = symmetric_residue<FOUR>(s, d0[i], d1[i], d2[i], d3[i]);
-        uint4 o;
-        o.x = pack4(r[0], r[1], r[2], r[3]);
-        o.y = pack4(r[4], r[5], r[6], r[7]);
-        o.z = pack4(r[8], r[9], r[10], r[11]);
-        o.w = pack4(r[12], r[13], r[14], r[15]);
-        *reinterpret_cast<uint4*>(reinterpret_cast<int8_t*>(dst) + (size_t)s * plane_stride) = o;
+    for (int s = 0; s < S; ++s) {
+        int r[E];
+#pragma unroll
+        for (int i = 0; i < E; ++i) r[i] = symmetric_residue<WIDE>(s, d0[i], d1[i], d2[i], d3[i]);
+        int8_t* o = dst + (size_t)s * plane_stride;
+        if (E == 16) {
+            *reinterpret_cast<uint4*>(o) = make_uint4(pack4(r[0], r[1], r[2], r[3]), pack4(r[4], r[5], r[6], r[7]),
+                                                      pack4(r[8], r[9], r[10], r[11]),
+                                                      pack4(r[12], r[13], r[14], r[15]));
+        } else {
+            *reinterpret_cast<uint2*>(o) = make_uint2(pack4(r[0], r[1], r[2], r[3]), pack4(r[4], r[5], r[6], r[7]));
+        }
     }
 }
 
@@ -369,35 +392,39 @@ __device__ __forceinline__ void slices16(const double (&vin)[16], int e, int bet
     }
 }
 
-// A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per 16
-// consecutive columns of a row (16-byte stores per plane, coalesced).
-template <int SCHEME, bool FOUR>
-__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A, long long rows, long long cols,
-                                                    const int32_t* __restrict__ shift, int S, int beta,
-                                                    int8_t* __restrict__ out, long long rows_p, long long cols_p) {
-    const long long chunks_per_row = cols_p >> 4;
+// A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per E
+// consecutive columns of a row (E = 8 for Scheme II, 8-byte stores per plane;
+// 16 for Scheme I), coalesced.  Scheme II is instantiated per slice count SC
+// (= S); Scheme I takes S at run time.
+template <int SCHEME, int SC, bool WIDE>
+__global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_rows(
+    const double* __restrict__ A, long long rows, long long cols, const int32_t* __restrict__ shift, int S, int beta,
+    int8_t* __restrict__ out, long long rows_p, long long cols_p) {
+    constexpr int E = SCHEME == 2 ? 8 : 16;
+    const long long chunks_per_row = cols_p / E;
     const long long total = rows_p * chunks_per_row;
     const size_t plane = (size_t)rows_p * (size_t)cols_p;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
          id += (long long)gridDim.x * blockDim.x) {
         const long long r = id / chunks_per_row;
-        const long long c0 = (id - r * chunks_per_row) << 4;
-        double v[16];
+        const long long c0 = (id - r * chunks_per_row) * E;
+        double v[E];
         int sh = 0;
         if (r < rows) {
             sh = shift[r];
             const double* src = A + r * cols + c0;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
+            for (int i = 0; i < E; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
         } else {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = 0.0;
+            for (int i = 0; i < E; ++i) v[i] = 0.0;
         }
-        uint4* dst = reinterpret_cast<uint4*>(out + (size_t)r * cols_p + c0);
+        int8_t* dst = out + (size_t)r * cols_p + c0;
         if (SCHEME == 2) {
-            residues16<FOUR>(v, sh, pow2_or_zero(sh), S, dst, plane);
+            residuesE<SC, WIDE, E>(v, sh, pow2_or_zero(sh), dst, plane);
         } else {
-            slices16(v, r < rows ? -sh : -1023, beta, S, dst, plane);
+            slices16(reinterpret_cast<const double(&)[16]>(v), r < rows ? -sh : -1023, beta, S,
+                     reinterpret_cast<uint4*>(dst), plane);
         }
     }
 }
@@ -405,8 +432,8 @@ __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ A
 // B (K x N, row-major) -> out[s][Np][Kp], i.e. B^T, K-major.  Tile of 128 k x
 // 32 n staged through shared memory; thread (n, kg) emits 16 consecutive k of
 // column n.  Also writes shift[n] = offset - max exponent of column n.
-template <int SCHEME, bool FOUR>
-__global__ void __launch_bounds__(256) k_slice_cols(const double* __restrict__ B, long long K, long long N,
+template <int SCHEME, int SC, bool WIDE>
+__global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const double* __restrict__ B, long long K, long long N,
                                                     const unsigned long long* __restrict__ colmax, int offset,
                                                     int S, int beta, int32_t* __restrict__ shift,
                                                     int8_t* __restrict__ out, long long Np, long long Kp) {
@@ -429,11 +456,11 @@ __global__ void __launch_bounds__(256) k_slice_cols(const double* __restrict__ B
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = tile[kg * 16 + i][lane];
     const size_t plane = (size_t)Np * (size_t)Kp;
-    uint4* dst = reinterpret_cast<uint4*>(out + (size_t)n * Kp + k0 + kg * 16);
+    int8_t* dst = out + (size_t)n * Kp + k0 + kg * 16;
     if (SCHEME == 2) {
-        residues16<FOUR>(v, sh, pow2_or_zero(sh), S, dst, plane);
+        residuesE<SC, WIDE, 16>(v, sh, pow2_or_zero(sh), dst, plane);
     } else {
-        slices16(v, e, beta, S, dst, plane);
+        slices16(v, e, beta, S, reinterpret_cast<uint4*>(dst), plane);
     }
 }
 
@@ -453,8 +480,8 @@ __device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t ma
 }
 
 // Running state of one element: T = sum c_s * (M / m_s) as NL 64-bit column
-// sums of 32-bit limb products (each below 2^45), and sum c_s * floor(2^24 / m_s)
-// for the quotient estimate.
+// sums of 32-bit limb products (each below 2^45), and a fixed-point estimate
+// of T / M (units of 2^-24, an underestimate by at most 0.07).
 template <int NL>
 struct CrtAcc {
     unsigned long long a[NL];
@@ -464,104 +491,126 @@ struct CrtAcc {
         for (int l = 0; l < NL; ++l) a[l] = 0ull;
         q = 0;
     }
+    // one residue s with coefficient c < m_s
     __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) {
 #pragma unroll
         for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)c * T.P[s][l];
         q += c * T.recip24[s];
     }
+    // residues 2p, 2p+1 with coefficients ca, cb: d = ca m_b + cb m_a < 2^17
+    __device__ __forceinline__ void add_pair(const CrtTable& T, int p, uint32_t ca, uint32_t cb) {
+        const uint32_t d = ca * c_mod[2 * p + 1].m + cb * c_mod[2 * p].m;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)d * T.PP[p][l];
+        q += d * T.precip24[p];
+    }
 };
 
-// x = T mod M, signed map at floor(M/2) (x >= floor(M/2) means -(M - x)), the
-// reference's conversion d0 + d1 2^64 + d2 2^128 over 64-bit limbs with a
-// rounding after each addition (crt_math.hpp:73-80), then ldexp(., -esum)
+// r = x - y over N 32-bit limbs.  The whole borrow chain is one asm block: the
+// carry flag does not survive between separate asm statements (the compiler
+// may schedule its own carry-using adds in between).
+template <int N>
+__device__ __forceinline__ void mw_sub(uint32_t (&r)[N], const uint32_t (&x)[N], const uint32_t (&y)[N]);
+
+template <>
+__device__ __forceinline__ void mw_sub<2>(uint32_t (&r)[2], const uint32_t (&x)[2], const uint32_t (&y)[2]) {
+    asm("sub.cc.u32 %0, %2, %4; subc.u32 %1, %3, %5;" : "=&r"(r[0]),"=&r"(r[1]) : "r"(x[0]),"r"(x[1]),"r"(y[0]),"r"(y[1]));
+}
+
+template <>
+__device__ __forceinline__ void mw_sub<3>(uint32_t (&r)[3], const uint32_t (&x)[3], const uint32_t (&y)[3]) {
+    asm("sub.cc.u32 %0, %3, %6; subc.cc.u32 %1, %4, %7; subc.u32 %2, %5, %8;" : "=&r"(r[0]),"=&r"(r[1]),"=&r"(r[2]) : "r"(x[0]),"r"(x[1]),"r"(x[2]),"r"(y[0]),"r"(y[1]),"r"(y[2]));
+}
+
+template <>
+__device__ __forceinline__ void mw_sub<4>(uint32_t (&r)[4], const uint32_t (&x)[4], const uint32_t (&y)[4]) {
+    asm("sub.cc.u32 %0, %4, %8; subc.cc.u32 %1, %5, %9; subc.cc.u32 %2, %6, %10; subc.u32 %3, %7, %11;" : "=&r"(r[0]),"=&r"(r[1]),"=&r"(r[2]),"=&r"(r[3]) : "r"(x[0]),"r"(x[1]),"r"(x[2]),"r"(x[3]),"r"(y[0]),"r"(y[1]),"r"(y[2]),"r"(y[3]));
+}
+
+template <>
+__device__ __forceinline__ void mw_sub<5>(uint32_t (&r)[5], const uint32_t (&x)[5], const uint32_t (&y)[5]) {
+    asm("sub.cc.u32 %0, %5, %10; subc.cc.u32 %1, %6, %11; subc.cc.u32 %2, %7, %12; subc.cc.u32 %3, %8, %13; subc.u32 %4, %9, %14;" : "=&r"(r[0]),"=&r"(r[1]),"=&r"(r[2]),"=&r"(r[3]),"=&r"(r[4]) : "r"(x[0]),"r"(x[1]),"r"(x[2]),"r"(x[3]),"r"(x[4]),"r"(y[0]),"r"(y[1]),"r"(y[2]),"r"(y[3]),"r"(y[4]));
+}
+
+template <>
+__device__ __forceinline__ void mw_sub<6>(uint32_t (&r)[6], const uint32_t (&x)[6], const uint32_t (&y)[6]) {
+    asm("sub.cc.u32 %0, %6, %12; subc.cc.u32 %1, %7, %13; subc.cc.u32 %2, %8, %14; subc.cc.u32 %3, %9, %15; subc.cc.u32 %4, %10, %16; subc.u32 %5, %11, %17;" : "=&r"(r[0]),"=&r"(r[1]),"=&r"(r[2]),"=&r"(r[3]),"=&r"(r[4]),"=&r"(r[5]) : "r"(x[0]),"r"(x[1]),"r"(x[2]),"r"(x[3]),"r"(x[4]),"r"(x[5]),"r"(y[0]),"r"(y[1]),"r"(y[2]),"r"(y[3]),"r"(y[4]),"r"(y[5]));
+}
+
+// x = T mod M mapped to [-(floor(M/2)+1), floor(M/2)) -- the reference's signed
+// map at floor(M/2) -- then its magnitude converted as the reference does,
+// d0 + d1 2^64 + d2 2^128 over 64-bit limbs with a rounding after each
+// addition (crt_math.hpp:73-80), sign applied, scaled by 2^-esum
 // (step4_reconstruction.hpp:59-184).
 template <int NL>
 __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>& acc, int esum) {
-    uint32_t t[NL + 1];
+    constexpr int L = NL + 1;
+    uint32_t t[L];
     unsigned long long carry = 0;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        unsigned long long v = acc.a[l] + carry;
+        const unsigned long long v = acc.a[l] + carry;
         t[l] = (uint32_t)v;
         carry = v >> 32;
     }
     t[NL] = (uint32_t)carry;
-    // q = floor(T / M) up to +-1: sum c_s floor(2^24/m_s) / 2^24 is within
-    // 20 * 255 / 2^24 of sum c_s / m_s = T / M.
-    const uint32_t q = acc.q >> 24;
-    uint32_t r[NL + 1];
-    long long borrow = 0;
-    unsigned long long qc = 0;
-#pragma unroll
-    for (int l = 0; l <= NL; ++l) {
-        unsigned long long qm = (unsigned long long)q * (l < NL ? T.M[l] : 0u) + qc;
-        qc = qm >> 32;
-        long long d = (long long)t[l] - (long long)(uint32_t)qm - borrow;
-        borrow = d < 0 ? 1 : 0;
-        r[l] = (uint32_t)d;
-    }
-    if (borrow) {   // q one too large: R += M
+    // nearest quotient: the estimate is q* or q* - 1, so V = T - q M is either
+    // the answer or the answer + M (then V >= floor(M/2)).
+    const uint32_t q = (acc.q + (1u << 23)) >> 24;
+    uint32_t qm[L];
+    {
         unsigned long long c = 0;
 #pragma unroll
-        for (int l = 0; l <= NL; ++l) {
-            unsigned long long v = (unsigned long long)r[l] + (l < NL ? T.M[l] : 0u) + c;
-            r[l] = (uint32_t)v;
+        for (int l = 0; l < L; ++l) {
+            const unsigned long long v = (unsigned long long)q * (l < NL ? T.M[l] : 0u) + c;
+            qm[l] = (uint32_t)v;
             c = v >> 32;
         }
-    } else {        // q one too small: R >= M, R -= M
-        bool ge = true;
-        if (r[NL] == 0) {
-#pragma unroll
-            for (int l = NL - 1; l >= 0; --l) {
-                if (r[l] != T.M[l]) {
-                    ge = r[l] > T.M[l];
-                    break;
-                }
-            }
-        }
-        if (ge) {
-            long long b = 0;
-#pragma unroll
-            for (int l = 0; l <= NL; ++l) {
-                long long d = (long long)r[l] - (long long)(l < NL ? T.M[l] : 0u) - b;
-                b = d < 0 ? 1 : 0;
-                r[l] = (uint32_t)d;
-            }
-        }
     }
-    bool neg = true;
+    uint32_t v[L], d[L], mh[L], m[L];
 #pragma unroll
-    for (int l = NL - 1; l >= 0; --l) {
-        if (r[l] != T.Mhalf[l]) {
-            neg = r[l] > T.Mhalf[l];
-            break;
-        }
+    for (int l = 0; l < L; ++l) {
+        mh[l] = l < NL ? T.Mhalf[l] : 0u;
+        m[l] = l < NL ? T.M[l] : 0u;
     }
+    mw_sub<L>(v, t, qm);
+    mw_sub<L>(d, v, mh);
+    if ((int)d[NL] >= 0) {      // V >= floor(M/2): one M too many
+        uint32_t w[L];
+        mw_sub<L>(w, v, m);
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[l] = w[l];
+    }
+    const bool neg = (int)v[NL] < 0;
     if (neg) {
-        long long b = 0;
+        uint32_t z[L];
 #pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            long long d = (long long)T.M[l] - (long long)r[l] - b;
-            b = d < 0 ? 1 : 0;
-            r[l] = (uint32_t)d;
-        }
+        for (int l = 0; l < L; ++l) z[l] = 0u;
+        uint32_t w[L];
+        mw_sub<L>(w, z, v);
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[l] = w[l];
     }
-    double mag = __ull2double_rn((unsigned long long)r[0] | (NL > 1 ? (unsigned long long)r[1] << 32 : 0ull));
+    double mag = __ull2double_rn((unsigned long long)v[0] | (NL > 1 ? (unsigned long long)v[1] << 32 : 0ull));
     if (NL > 2) {
-        unsigned long long w1 = (unsigned long long)r[2] | (NL > 3 ? (unsigned long long)r[3] << 32 : 0ull);
+        const unsigned long long w1 = (unsigned long long)v[2] | (NL > 3 ? (unsigned long long)v[3] << 32 : 0ull);
         mag = __dadd_rn(mag, __ull2double_rn(w1) * 0x1p64);
     }
-    if (NL > 4) mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)r[4]) * 0x1p128);
-    return ldexp(neg ? -mag : mag, -esum);
+    if (NL > 4) mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)v[4]) * 0x1p128);
+    const int e = -esum;
+    return scale_pow2(neg ? -mag : mag, e, pow2_or_zero(e));
 }
 
 // ---------------------------------------------------------------------------
 // Step 3: tcgen05 INT8 GEMM
 // ---------------------------------------------------------------------------
-// One persistent CTA per SM walks output tiles (128 x 256); for each tile it
-// runs every group g (Scheme II: residue g, A_g * B_g^T; Scheme I: the slice
-// pairs with s + t = g + 2) into one of two TMEM accumulators, so the
-// epilogue of unit (tile, g) overlaps the MMAs of unit (tile, g + 1).
+// One persistent CTA per SM walks work units (group g, output tile 128 x 256)
+// in group-major order, round-robin over CTAs (Scheme II: residue g,
+// A_g * B_g^T; Scheme I: the slice pairs with s + t = g + 2).  Each unit
+// accumulates into one of two TMEM accumulators, so the epilogue of one unit
+// overlaps the MMAs of the next.  Group-major order keeps the CTAs on the
+// same pair of planes at a time (L2-resident); a tile-major order made them
+// drift across all S planes and re-read them from HBM (4.6x at 8192^3, S=16).
 //   warp 0      TMA producer (4-stage ring of A 128x128 + B^T 256x128 int8 tiles)
 //   warp 1      TMEM allocation, UMMA issue (one elected lane)
 //   warps 2..9  epilogue; warp w reads TMEM lanes 32 (w % 4).. and column half (w - 2) / 4
@@ -593,9 +642,7 @@ struct GemmArgs {
 
 // Tile t -> (mt, nt).  Tiles are walked in bands of `band` m-tiles, n-major
 // inside a band, so the ~148 tiles in flight at once cover a band x (148/band)
-// block: per residue plane they touch band * 1 MB of A and 148/band * 2 MB of
-// B^T (at K = 8192), which stays L2-resident while every CTA cycles through
-// the S planes of its own tile.
+// block: band * 1 MB of A and 148/band * 2 MB of B^T at K = 8192.
 __device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, int& nt) {
     const int per_band = a.band * a.n_tiles;
     const int b = t / per_band;
@@ -646,6 +693,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    const int total_units = G * args.total_tiles;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -653,10 +701,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint32_t phase = 0;
         long long issued = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+        for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
+            const int grp = u / args.total_tiles;
             int mt, nt;
-            tile_coords(t, args, mt, nt);
-            for (int grp = 0; grp < G && ok; ++grp) {
+            tile_coords(u - grp * args.total_tiles, args, mt, nt);
+            {
                 for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
                     const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kTileM);
                     const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN);
@@ -696,8 +745,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint32_t phase = 0;
         int local = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
-            for (int grp = 0; grp < G && ok; ++grp, ++local) {
+        for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
+            const int grp = u / args.total_tiles;
+            {
                 const int acc = local & 1;
                 const uint32_t acc_phase = (local >> 1) & 1;
                 int w = 1;
@@ -751,18 +801,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const int row_local = q * 32 + lane;
         int local = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+        for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
+            const int grp = u / args.total_tiles;
             int mt, nt;
-            tile_coords(t, args, mt, nt);
+            tile_coords(u - grp * args.total_tiles, args, mt, nt);
             const long long row = (long long)mt * kTileM + row_local;
-            for (int grp = 0; grp < G; ++grp, ++local) {
+            {
                 const int acc = local & 1;
                 const uint32_t acc_phase = (local >> 1) & 1;
                 int w = 1;
                 if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
                 if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
                     ok = false;
-                    break;
+                    continue;
                 }
                 tc_fence_after();
                 const uint32_t taddr =
@@ -829,11 +880,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 // Scheme II step 4 from the coefficient byte planes [S][Mp][Np] written by the
 // GEMM epilogue: one thread per 4 consecutive columns of a row (a warp reads
 // 128 contiguous bytes per plane), exact CRT per element, FP64 C.  Few
-// registers per thread, so the multiword arithmetic runs at full occupancy.
-template <int NL>
+// registers per thread, so the multiword arithmetic runs at full occupancy;
+// with S fixed at compile time the table constants are instruction operands
+// and the S loads are issued together.
+template <int S>
 __global__ void __launch_bounds__(256) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
-                                                  long long M, long long N, int S, const int32_t* __restrict__ sA,
+                                                  long long M, long long N, const int32_t* __restrict__ sA,
                                                   const int32_t* __restrict__ sB, double* __restrict__ C) {
+    constexpr int NL = (S + 3) / 4;   // 32-bit limbs of M
     const long long chunks = (N + 3) >> 2;
     const long long total = M * chunks;
     const size_t plane = (size_t)Mp * (size_t)Np;
@@ -842,13 +896,21 @@ __global__ void __launch_bounds__(256) k_crt_coef(const uint8_t* __restrict__ co
          id += (long long)gridDim.x * blockDim.x) {
         const long long i = id / chunks, j0 = (id - i * chunks) << 2;
         const uint8_t* src = coef + (size_t)i * Np + j0;
+        uint32_t w[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) w[s] = __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)s * plane));
         CrtAcc<NL> st[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) st[e].zero();
-        for (int s = 0; s < S; ++s) {
-            const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)s * plane));
 #pragma unroll
-            for (int e = 0; e < 4; ++e) st[e].add(T, s, (w >> (e * 8)) & 0xFFu);
+        for (int p = 0; p < S / 2; ++p) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                st[e].add_pair(T, p, (w[2 * p] >> (e * 8)) & 0xFFu, (w[2 * p + 1] >> (e * 8)) & 0xFFu);
+        }
+        if (S & 1) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) st[e].add(T, S - 1, (w[S - 1] >> (e * 8)) & 0xFFu);
         }
         const int sa = sA[i];
         double* crow = C + i * N;
@@ -978,19 +1040,33 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
     return cudaGetLastError();
 }
 
+// Scheme II slicers are instantiated per slice count; WIDE digit splitting is
+// needed only when K_param > 62, which requires S >= 17.
+#define OZA_FOR_EACH_S(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) \
+    X(16) X(17) X(18) X(19) X(20)
+
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift, int S,
-                              int beta, int8_t* out, size_t rows_p, size_t cols_p, int sms, cudaStream_t st) {
-    long long chunks = (long long)rows_p * (long long)(cols_p / 16);
+                              int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
+                              cudaStream_t st) {
+    long long chunks = (long long)rows_p * (long long)(cols_p / (scheme == 2 ? 8 : 16));
     if (chunks == 0) return cudaSuccess;
-    int grid = grid_for(chunks, 256, sms);
-    if (scheme == 2) {
-        // rint(ldexp(x, shift)) is below 2^(K_param) in magnitude; four radix-2^21
-        // digits are needed only once K_param exceeds 62.
-        k_slice_rows<2, true><<<grid, 256, 0, st>>>(A, (long long)rows, (long long)cols, shift, S, 0, out,
-                                                    (long long)rows_p, (long long)cols_p);
-    } else {
-        k_slice_rows<1, false><<<grid, 256, 0, st>>>(A, (long long)rows, (long long)cols, shift, S, beta, out,
-                                                     (long long)rows_p, (long long)cols_p);
+    const int grid = grid_for(chunks, 256, sms);
+    const long long R = (long long)rows, C = (long long)cols, RP = (long long)rows_p, CP = (long long)cols_p;
+    if (scheme == 1) {
+        k_slice_rows<1, 0, false><<<grid, 256, 0, st>>>(A, R, C, shift, S, beta, out, RP, CP);
+        return cudaGetLastError();
+    }
+    const bool wide = k_param > 62;
+    if (wide && S < 17) return cudaErrorInvalidValue;   // K_param <= 61 for S <= 16
+    switch (S) {
+#define OZA_CASE(n)                                                                                   \
+    case n:                                                                                           \
+        if (wide) k_slice_rows<2, n, (n >= 17)><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP); \
+        else k_slice_rows<2, n, false><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP);         \
+        break;
+        OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+        default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
@@ -999,13 +1075,23 @@ cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, c
                               int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
                               cudaStream_t st) {
     if (Np == 0 || Kp == 0) return cudaSuccess;
-    dim3 grid((unsigned)(Np / 32), (unsigned)(Kp / 128));
-    if (scheme == 2) {
-        k_slice_cols<2, true><<<grid, 256, 0, st>>>(B, (long long)K, (long long)N, colmax, offset, S, 0, shift, out,
-                                                    (long long)Np, (long long)Kp);
-    } else {
-        k_slice_cols<1, false><<<grid, 256, 0, st>>>(B, (long long)K, (long long)N, colmax, offset, S, beta, shift,
-                                                     out, (long long)Np, (long long)Kp);
+    const dim3 grid((unsigned)(Np / 32), (unsigned)(Kp / 128));
+    const long long KK = (long long)K, NN = (long long)N, NP = (long long)Np, KP = (long long)Kp;
+    if (scheme == 1) {
+        k_slice_cols<1, 0, false><<<grid, 256, 0, st>>>(B, KK, NN, colmax, offset, S, beta, shift, out, NP, KP);
+        return cudaGetLastError();
+    }
+    const bool wide = offset > 62;
+    if (wide && S < 17) return cudaErrorInvalidValue;
+    switch (S) {
+#define OZA_CASE(n)                                                                                          \
+    case n:                                                                                                  \
+        if (wide) k_slice_cols<2, n, (n >= 17)><<<grid, 256, 0, st>>>(B, KK, NN, colmax, offset, n, 0, shift, out, NP, KP); \
+        else k_slice_cols<2, n, false><<<grid, 256, 0, st>>>(B, KK, NN, colmax, offset, n, 0, shift, out, NP, KP);         \
+        break;
+        OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+        default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
@@ -1070,13 +1156,14 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
                             const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st) {
     long long total = (long long)M * (long long)((N + 3) / 4);
     if (total == 0) return cudaSuccess;
-    int grid = grid_for(total, 256, sms, 16);
-    switch ((S + 3) / 4) {   // 32-bit limbs of M
-        case 1: k_crt_coef<1><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
-        case 2: k_crt_coef<2><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
-        case 3: k_crt_coef<3><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
-        case 4: k_crt_coef<4><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
-        default: k_crt_coef<5><<<grid, 256, 0, st>>>(coef, Mp, Np, M, N, S, shiftA, shiftB, C); break;
+    const int grid = grid_for(total, 256, sms, 16);
+    const long long MP = (long long)Mp, NP = (long long)Np, MM = (long long)M, NN = (long long)N;
+    switch (S) {
+#define OZA_CASE(n) \
+    case n: k_crt_coef<n><<<grid, 256, 0, st>>>(coef, MP, NP, MM, NN, shiftA, shiftB, C); break;
+        OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+        default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

@@ -42,7 +42,7 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 // scheme 2: symmetric residues of rint(ldexp(x, shift)).
 // Rows: A (rows x cols, row-major) -> out[s][rows_p][cols_p].
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift,
-                              int S, int beta, int8_t* out, size_t rows_p, size_t cols_p, int sms,
+                              int S, int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
                               cudaStream_t st);
 // Columns: B (K x N, row-major) -> out[s][Np][Kp] (transposed, K-major); also
 // writes shift[n] = offset - max exponent of column n.
