@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=8192)
+    p.add_argument("--mnk", type=str, default=None, help="M,N,K for a rectangular GEMM (overrides --size)")
     p.add_argument("--slices", type=int, default=16)
     p.add_argument("--scheme", type=int, default=2, choices=[1, 2])
     p.add_argument("--phi", type=float, default=0.5)
@@ -56,18 +57,31 @@ def parse():
     return p.parse_args()
 
 
+def dims(args):
+    if args.mnk:
+        M, N, K = (int(x) for x in args.mnk.split(","))
+        return M, N, K
+    return args.size, args.size, args.size
+
+
 def workload(args):
-    return {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{args.size}^3",
-            "M": args.size, "N": args.size, "K": args.size, "scheme": args.scheme,
+    M, N, K = dims(args)
+    shape = f"{M}^3" if M == N == K else f"{M}x{N}x{K}"
+    return {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{shape}",
+            "M": M, "N": N, "K": K, "scheme": args.scheme,
             "slices": args.slices, "phi": args.phi, "input_seeds": [42, 43],
             "path": "materialized" if getattr(args, "materialize", False) else "fused",
-            "layout": "row-major fp64", "l2": "inputs (1 GiB) larger than L2; no flush"}
+            "layout": "row-major fp64",
+            "l2": f"inputs ({(M * K + K * N) * 8 / 2**30:.2f} GiB) "
+                  + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
+                     "fit in L2: timings include L2 reuse")}
 
 
 def int8_ops(args):
     S = args.slices
     G = S if args.scheme == 2 else S * (S + 1) // 2
-    return 2.0 * args.size ** 3 * G
+    M, N, K = dims(args)
+    return 2.0 * M * N * K * G
 
 
 # ------------------------------------------------------------------ distributed
@@ -241,10 +255,9 @@ def run_reference_arm(args, ws, rank):
         return
     import numpy as np
     import ozablas_b200 as oz
-    n = args.size
-    A = oz.generate_matrix(min(args.cpu_sample, n), n, args.phi, 42)
-    Bfull_cols = min(args.cpu_sample, n)
-    B = oz.generate_matrix(n, n, args.phi, 43)[:, :Bfull_cols] if n <= 8192 else None
+    M, N, K = dims(args)
+    A = oz.generate_matrix(min(args.cpu_sample, M), K, args.phi, 42)
+    B = oz.generate_matrix(K, N, args.phi, 43)[:, :min(args.cpu_sample, N)]
     res = cpu_reference_sample(args, A, np.ascontiguousarray(B), steps=args.steps, warmup=min(args.warmup, 1))
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["seconds_per_sample"] * 1e3, "higher_is_better": True,
@@ -291,18 +304,19 @@ def run_ours(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    n, S = args.size, args.slices
-    hA = oz.generate_matrix(n, n, args.phi, 42)
-    hB = oz.generate_matrix(n, n, args.phi, 43)
+    M, N, K = dims(args)
+    S = args.slices
+    hA = oz.generate_matrix(M, K, args.phi, 42)
+    hB = oz.generate_matrix(K, N, args.phi, 43)
     pA = torch.from_numpy(hA).pin_memory()
     pB = torch.from_numpy(hB).pin_memory()
     dA = pA.to(dev)
     dB = pB.to(dev)
-    dC = torch.empty(n, n, dtype=torch.float64, device=dev)
+    dC = torch.empty(M, N, dtype=torch.float64, device=dev)
     ex = oz.CudaExecutor(local)
     stream = torch.cuda.current_stream(dev)
     ex.set_stream(stream.cuda_stream)
-    W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, n, n, n, S,
+    W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, M, N, K, S,
                                                                          materialize=args.materialize)
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
@@ -315,7 +329,7 @@ def run_ours(args, ws, rank, local):
         ms = time_events(step, args.steps, stream)
     barrier(ws)
     ms = dist_max(ms, ws)
-    flops = 2.0 * n ** 3
+    flops = 2.0 * M * N * K
     value = ws * flops / (ms * 1e-3) / 1e12
 
     # per-step breakdown and the GEMM kernel's own duration (events around the launch)
@@ -329,7 +343,7 @@ def run_ours(args, ws, rank, local):
     step_ms = dict(zip(("step1_ms", "step2_ms", "step3_ms", "step4_ms", "total_ms"), acc))
 
     # end to end through the public API: host buffers, copies inside the timed region
-    hC = torch.empty(n, n, dtype=torch.float64).pin_memory()
+    hC = torch.empty(M, N, dtype=torch.float64).pin_memory()
 
     def e2e_step():
         dA.copy_(pA, non_blocking=True)
@@ -349,12 +363,12 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and not args.no_extras:
         # cuBLAS INT8 GEMM (torch._int_mm) at the same size, for the INT8 peak reference
         try:
-            a8 = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
-            b8 = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=dev)
+            a8 = torch.randint(-128, 127, (M, K), dtype=torch.int8, device=dev)
+            b8 = torch.randint(-128, 127, (K, N), dtype=torch.int8, device=dev)
             for _ in range(3):
                 torch._int_mm(a8, b8)
             i8ms = time_events(lambda: torch._int_mm(a8, b8), 10, stream)
-            extras["cublas_int8_tops"] = 2.0 * n ** 3 / (i8ms * 1e-3) / 1e12
+            extras["cublas_int8_tops"] = flops / (i8ms * 1e-3) / 1e12
             del a8, b8
         except Exception as e:  # noqa: BLE001
             extras["cublas_int8_tops"] = f"unavailable: {e}"
@@ -379,9 +393,9 @@ def run_ours(args, ws, rank, local):
 
     gemm_ms = step_ms["step3_ms"]
     achieved = int8_ops(args) / (gemm_ms * 1e-3) / 1e12
-    traffic = load_traffic().get(f"gemm_i8_{n}_S{S}_scheme{args.scheme}")
-    bytes_h2d = 2 * n * n * 8
-    bytes_d2h = n * n * 8
+    traffic = load_traffic().get(workload(args)["workload"] + f"_S{S}")
+    bytes_h2d = (M * K + K * N) * 8
+    bytes_d2h = M * N * 8
     steps_kernels = 6
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -422,8 +436,8 @@ def reference_gpu_tflops(args, dA, dB, stream):
     so = os.path.join(ROOT, "baseline", "_ref", "libozablas_ref_gpu.so")
     if not os.path.exists(so):
         return "unavailable: baseline/_ref not built"
-    n = args.size
-    if args.scheme == 2 and args.slices * n * n >= 2 ** 31:
+    M, N, K = dims(args)
+    if max(M * K, K * N, M * N) * args.slices >= 2 ** 31:
         return "unavailable: the reference's 32-bit index arithmetic overflows at this size"
     L = ctypes.CDLL(so)
     L.refgpu_init.argtypes = [ctypes.c_int]
@@ -433,10 +447,10 @@ def reference_gpu_tflops(args, dA, dB, stream):
     L.refgpu_ws_destroy.argtypes = [ctypes.c_void_p]
     if L.refgpu_init(torch.cuda.current_device()) != 0:
         return "unavailable: executor init failed"
-    h = L.refgpu_ws_create(args.scheme, n, n, n, args.slices)
+    h = L.refgpu_ws_create(args.scheme, M, N, K, args.slices)
     if not h:
         return "unavailable: workspace allocation failed"
-    dR = torch.empty(n, n, dtype=torch.float64, device=dA.device)
+    dR = torch.empty(M, N, dtype=torch.float64, device=dA.device)
     # the reference issues on the legacy default stream
     torch.cuda.synchronize()
     run = lambda: L.refgpu_gemm(h, dA.data_ptr(), dB.data_ptr(), dR.data_ptr(), None)  # noqa: E731
@@ -450,7 +464,7 @@ def reference_gpu_tflops(args, dA, dB, stream):
     torch.cuda.synchronize()
     ms = (time.perf_counter() - t0) / reps * 1e3
     L.refgpu_ws_destroy(h)
-    return 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+    return 2.0 * M * N * K / (ms * 1e-3) / 1e12
 
 
 def main():

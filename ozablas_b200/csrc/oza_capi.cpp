@@ -73,6 +73,7 @@ struct oza_workspace {
     int32_t* ctc = nullptr;          // INT32 group planes (materialised / Scheme I)
     uint8_t* coef = nullptr;         // Scheme II CRT coefficient bytes [S][Mp][Np]
     bool fused = false;
+    bool pair = false;               // GEMM on CTA pairs (cta_group::2)
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     oza::PairList pairs{};
@@ -240,7 +241,9 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     ws->M = M;
     ws->N = N;
     ws->K = K;
-    ws->Mp = oza::round_up(M, oza::kTileM);
+    // CTA-pair kernel (256-row tiles) unless A has at most 128 rows.
+    ws->pair = M > (size_t)oza::kTileM;
+    ws->Mp = oza::round_up(M, ws->pair ? oza::kTileMPair : oza::kTileM);
     ws->Np = oza::round_up(N, oza::kTileN);
     ws->Kp = oza::round_up(K, oza::kTileK);
     ws->groups = slices;
@@ -401,6 +404,7 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
+        plan.pair = ws->pair;
         plan.ctc = ws->ctc;
         plan.coef = ws->fused ? ws->coef : nullptr;
         OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");

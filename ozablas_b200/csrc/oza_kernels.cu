@@ -98,7 +98,17 @@ cudaError_t upload_tables() {
         mc[s].c21 = sym_rep(pow2_mod(21, m), m);
         mc[s].c42 = sym_rep(pow2_mod(42, m), m);
         mc[s].c63 = sym_rep(pow2_mod(63, m), m);
-        mc[s].pad = 0;
+        mc[s].magic32 = (uint32_t)(((1ull << 32) + m - 1) / m);
+        mc[s].bh = (int32_t)(m * 1024 + (m - 1) / 2);
+        mc[s].adj = (int32_t)(256 - (m - 1) / 2);
+        for (int w = 0; w < 4; ++w) {
+            uint32_t word = 0;
+            for (int b = 0; b < 4; ++b) {
+                const int32_t c = sym_rep(pow2_mod(8 * (4 * w + b), m), m);
+                word |= (uint32_t)(uint8_t)(int8_t)c << (8 * b);
+            }
+            mc[s].dig[w] = word;
+        }
     }
     for (int S = 1; S <= kMaxSlices; ++S) {
         CrtTable& t = ct[S - 1];
@@ -339,24 +349,61 @@ __device__ __forceinline__ int cvt_s8(double v) {
 // Scheme II residues of E (8 or 16) consecutive values: plane s of dst receives
 // the E packed residues modulo m_s (reference slice_scheme2_A/B,
 // step2_slicing.hpp:110-206: x = rint(ldexp(v, shift)), symmetric residues).
+//
+// NARROW (K_param <= 62, so |x| <= 2^62): x = sum_{i<8} d_i 256^i with signed
+// byte digits d_i = byte_i(x + 0x8080...80) - 128, and
+//   u = m 2^10 + (m-1)/2 + sum_i d_i (256^i mod m)       (two dp4a)
+// lies in (0, 2^19); q = umulhi(u, ceil(2^32/m)) = floor(u/m) exactly (u m <
+// 2^32) and the low byte of u - q m + 256 - (m-1)/2 is the symmetric residue.
+// WIDE (|x| < 2^84): radix-2^21 digits and the magic division of
+// symmetric_residue.
 template <int S, bool WIDE, int E>
 __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p, int8_t* dst, size_t plane_stride) {
+    if (!WIDE) {
+        int dlo[E], dhi[E];
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const double x = rint(scale_pow2(v[i], sh, p));
+            const unsigned long long t = (unsigned long long)__double2ll_rn(x);
+            const unsigned long long w = (t + 0x8080808080808080ull) ^ 0x8080808080808080ull;
+            dlo[i] = (int)(uint32_t)w;
+            dhi[i] = (int)(uint32_t)(w >> 32);
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const ModConst& mc = c_mod[s];
+            uint32_t r[E];
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const uint32_t u = (uint32_t)__dp4a(dhi[i], (int)mc.dig[1], __dp4a(dlo[i], (int)mc.dig[0], mc.bh));
+                r[i] = u - __umulhi(u, mc.magic32) * mc.m + (uint32_t)mc.adj;
+            }
+            uint32_t wds[E / 4];
+#pragma unroll
+            for (int k = 0; k < E / 4; ++k)
+                wds[k] = __byte_perm(__byte_perm(r[4 * k], r[4 * k + 1], 0x3340),
+                                     __byte_perm(r[4 * k + 2], r[4 * k + 3], 0x3340), 0x5410);
+            int8_t* o = dst + (size_t)s * plane_stride;
+            if constexpr (E == 16) *reinterpret_cast<uint4*>(o) = make_uint4(wds[0], wds[1], wds[2], wds[3]);
+            else *reinterpret_cast<uint2*>(o) = make_uint2(wds[0], wds[1]);
+        }
+        return;
+    }
     int d0[E], d1[E], d2[E], d3[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const double x = rint(scale_pow2(v[i], sh, p));
-        split21<WIDE>(x, d0[i], d1[i], d2[i], d3[i]);
+        split21<true>(x, d0[i], d1[i], d2[i], d3[i]);
     }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int r[E];
 #pragma unroll
-        for (int i = 0; i < E; ++i) r[i] = symmetric_residue<WIDE>(s, d0[i], d1[i], d2[i], d3[i]);
+        for (int i = 0; i < E; ++i) r[i] = symmetric_residue<true>(s, d0[i], d1[i], d2[i], d3[i]);
         int8_t* o = dst + (size_t)s * plane_stride;
-        if (E == 16) {
+        if constexpr (E == 16) {
             *reinterpret_cast<uint4*>(o) = make_uint4(pack4(r[0], r[1], r[2], r[3]), pack4(r[4], r[5], r[6], r[7]),
-                                                      pack4(r[8], r[9], r[10], r[11]),
-                                                      pack4(r[12], r[13], r[14], r[15]));
+                                                      pack4(r[8], r[9], r[10], r[11]), pack4(r[12], r[13], r[14], r[15]));
         } else {
             *reinterpret_cast<uint2*>(o) = make_uint2(pack4(r[0], r[1], r[2], r[3]), pack4(r[4], r[5], r[6], r[7]));
         }
@@ -652,6 +699,52 @@ __device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, i
     mt = b * a.band + (tb - nt * rows);
 }
 
+// One work unit's epilogue for one warp: 32 TMEM lanes (rows) x 128 columns
+// (`half` of the 256-column accumulator at taddr) of output tile column nt.
+template <int EPI>
+__device__ __forceinline__ void epilogue_unit(const GemmArgs& args, uint32_t taddr, long long row, int grp, int nt,
+                                              int half) {
+    if (EPI == kEpiI32) {
+        int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+                       (size_t)nt * kTileN + half * (kTileN / 2);
+#pragma unroll 1
+        for (int c = 0; c < kTileN / 64; ++c) {
+            uint32_t r[32];
+            tmem_ld32(taddr + c * 32, r);
+            tmem_ld_wait();
+            int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+#pragma unroll
+            for (int v = 0; v < 8; ++v)
+                d4[v] = make_int4((int)r[4 * v], (int)r[4 * v + 1], (int)r[4 * v + 2], (int)r[4 * v + 3]);
+        }
+    } else {
+        // Scheme II: reduce each INT32 residue product to its CRT
+        // coefficient ((C mod m_g) * inv_g) mod m_g, one byte.
+        const ModConst mc = c_mod[grp];
+        const uint32_t inv = c_crt[args.S - 1].inv[grp], c16 = c_crt[args.S - 1].c16inv[grp];
+        uint8_t* dst = args.coef + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+                       (size_t)nt * kTileN + half * (kTileN / 2);
+#pragma unroll 1
+        for (int c = 0; c < kTileN / 64; ++c) {
+            uint32_t r[32];
+            tmem_ld32(taddr + c * 32, r);
+            tmem_ld_wait();
+            uint32_t wds[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                uint32_t b0 = crt_coeff((int32_t)r[4 * v], mc.m, mc.magic, inv, c16);
+                uint32_t b1 = crt_coeff((int32_t)r[4 * v + 1], mc.m, mc.magic, inv, c16);
+                uint32_t b2 = crt_coeff((int32_t)r[4 * v + 2], mc.m, mc.magic, inv, c16);
+                uint32_t b3 = crt_coeff((int32_t)r[4 * v + 3], mc.m, mc.magic, inv, c16);
+                wds[v] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+            }
+            uint4* d4 = reinterpret_cast<uint4*>(dst + c * 32);
+            d4[0] = make_uint4(wds[0], wds[1], wds[2], wds[3]);
+            d4[1] = make_uint4(wds[4], wds[5], wds[6], wds[7]);
+        }
+    }
+}
+
 template <int EPI>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -818,45 +911,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 tc_fence_after();
                 const uint32_t taddr =
                     tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-                if (EPI == kEpiI32) {
-                    int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
-                                   (size_t)nt * kTileN + half * (kTileN / 2);
-#pragma unroll 1
-                    for (int c = 0; c < kTileN / 64; ++c) {
-                        uint32_t r[32];
-                        tmem_ld32(taddr + c * 32, r);
-                        tmem_ld_wait();
-                        int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
-#pragma unroll
-                        for (int v = 0; v < 8; ++v)
-                            d4[v] = make_int4((int)r[4 * v], (int)r[4 * v + 1], (int)r[4 * v + 2], (int)r[4 * v + 3]);
-                    }
-                } else {
-                    // Scheme II: reduce each INT32 residue product to its CRT
-                    // coefficient ((C mod m_g) * inv_g) mod m_g, one byte.
-                    const ModConst mc = c_mod[grp];
-                    const uint32_t inv = c_crt[args.S - 1].inv[grp], c16 = c_crt[args.S - 1].c16inv[grp];
-                    uint8_t* dst = args.coef + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
-                                   (size_t)nt * kTileN + half * (kTileN / 2);
-#pragma unroll 1
-                    for (int c = 0; c < kTileN / 64; ++c) {
-                        uint32_t r[32];
-                        tmem_ld32(taddr + c * 32, r);
-                        tmem_ld_wait();
-                        uint32_t wds[8];
-#pragma unroll
-                        for (int v = 0; v < 8; ++v) {
-                            uint32_t b0 = crt_coeff((int32_t)r[4 * v], mc.m, mc.magic, inv, c16);
-                            uint32_t b1 = crt_coeff((int32_t)r[4 * v + 1], mc.m, mc.magic, inv, c16);
-                            uint32_t b2 = crt_coeff((int32_t)r[4 * v + 2], mc.m, mc.magic, inv, c16);
-                            uint32_t b3 = crt_coeff((int32_t)r[4 * v + 3], mc.m, mc.magic, inv, c16);
-                            wds[v] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
-                        }
-                        uint4* d4 = reinterpret_cast<uint4*>(dst + c * 32);
-                        d4[0] = make_uint4(wds[0], wds[1], wds[2], wds[3]);
-                        d4[1] = make_uint4(wds[4], wds[5], wds[6], wds[7]);
-                    }
-                }
+                epilogue_unit<EPI>(args, taddr, row, grp, nt, half);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -876,6 +931,203 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 // ---------------------------------------------------------------------------
 // Step 4: reconstruction
 // ---------------------------------------------------------------------------
+
+// ---------------------------------------------------------------------------
+// Step 3 on CTA pairs: tcgen05.mma.cta_group::2, 256 x 256 output tiles
+// ---------------------------------------------------------------------------
+// Same work units and epilogues as k_gemm_i8, but a cluster of two CTAs on two
+// SMs computes a 256 x 256 tile with M = 256 UMMAs: each CTA stages its own
+// 128 rows of A and its own 128-row half of B^T (16 + 16 KB per stage, 6
+// stages), so per SM the operand traffic per MAC is 2/3 of the one-CTA
+// 128 x 256 tile.  The even CTA issues the MMAs; TMA completions of both CTAs
+// are counted on its full barriers; MMA commits arrive on both CTAs'
+// barriers; both CTAs' epilogue warps release the accumulator on the even
+// CTA's acc_empty barrier.  No TMA multicast is used.
+constexpr int kPairStages = 6;
+constexpr int kPairTileM = 256;                   // rows of C per CTA pair
+constexpr int kPairABytes = 128 * kTileK;         // this CTA's 128 rows of A
+constexpr int kPairBBytes = 128 * kTileK;         // this CTA's half of B^T
+constexpr int kPairSmem = kPairStages * (kPairABytes + kPairBBytes) + 1024 + 256;
+
+template <int EPI>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
+    k_gemm_i8_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ PairList pairs, const GemmArgs args) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + kPairStages * kPairABytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + kPairStages * kPairBBytes);
+    uint64_t* empty = full + kPairStages;
+    uint64_t* acc_full = empty + kPairStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = rank == 0;
+    const int pair_id = blockIdx.x >> 1, num_pairs = gridDim.x >> 1;
+    const int G = args.groups;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kPairStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&acc_full[0], 1);
+        mbar_init(&acc_full[1], 1);
+        mbar_init(&acc_empty[0], 2 * kEpiWarps);
+        mbar_init(&acc_empty[1], 2 * kEpiWarps);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc_pair(tmem_slot, kTmemCols);
+        tmem_relinquish_pair();
+    }
+    tc_fence_before();
+    cluster_sync();   // barriers of both CTAs initialised before any remote signal
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total_units = G * args.total_tiles;
+
+    if (warp == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        int stage = 0;
+        uint32_t phase = 0;
+        bool ok = true;
+        for (int u = pair_id; u < total_units && ok; u += num_pairs) {
+            const int grp = u / args.total_tiles;
+            int mt, nt;
+            tile_coords(u - grp * args.total_tiles, args, mt, nt);
+            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kPairTileM + rank * 128);
+                const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN + rank * 128);
+                for (int kb = 0; kb < args.k_blocks; ++kb) {
+                    int w = 1;
+                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
+                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                    if (!ok) break;
+                    if (lane == 0) {
+                        const uint32_t fbar = mapa_shared(smem_u32(&full[stage]), 0);
+                        if (leader) mbar_arrive_expect_tx(&full[stage], 2 * (kPairABytes + kPairBBytes));
+                        tma_load_2d_pair(sA + stage * kPairABytes, &tmA, fbar, kb * kTileK, arow);
+                        tma_load_2d_pair(sB + stage * kPairBBytes, &tmB, fbar, kb * kTileK, brow);
+                    }
+                    __syncwarp();
+                    if (++stage == kPairStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+        }
+        if (!ok && leader && lane == 0) {
+            // Let the copies of both CTAs land (the leader's full barriers count them).
+            volatile int no_abort = 0;
+            for (int j = 0; j < kPairStages; ++j) {
+                int st = (stage + kPairStages - 1 - j) % kPairStages;
+                uint32_t ph = (st < stage) ? phase : (phase ^ 1);
+                mbar_wait(&full[st], ph, &no_abort, nullptr);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer (even CTA) ----------------
+        if (leader) {
+            constexpr uint32_t idesc = umma_idesc_i8(kPairTileM, kTileN);
+            int stage = 0;
+            uint32_t phase = 0;
+            int local = 0;
+            bool ok = true;
+            for (int u = pair_id; u < total_units && ok; u += num_pairs, ++local) {
+                const int grp = u / args.total_tiles;
+                const int acc = local & 1;
+                const uint32_t acc_phase = (local >> 1) & 1;
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
+                ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + acc * kAccCols;
+                uint32_t accumulate = 0;
+                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                    for (int kb = 0; kb < args.k_blocks; ++kb) {
+                        w = 1;
+                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
+                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                        if (!ok) break;
+                        tc_fence_after();
+                        if (lane == 0) {
+                            const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kPairABytes));
+                            const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kPairBBytes));
+#pragma unroll
+                            for (int k = 0; k < kTileK / 32; ++k) {
+                                umma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
+                                accumulate = 1;
+                            }
+                            umma_commit_pair(&empty[stage]);
+                        }
+                        __syncwarp();
+                        accumulate = 1;
+                        if (++stage == kPairStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+                if (!ok) break;
+                if (lane == 0) umma_commit_pair(&acc_full[acc]);
+                __syncwarp();
+            }
+            if (!ok && lane == 0) {
+                umma_commit_pair(drain);
+                volatile int no_abort = 0;
+                mbar_wait(drain, 0, &no_abort, nullptr);
+            }
+        }
+    } else {
+        // ---------------- epilogue (both CTAs, own TMEM) ----------------
+        const int q = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int row_local = q * 32 + lane;
+        const uint32_t empty_remote[2] = {mapa_shared(smem_u32(&acc_empty[0]), 0),
+                                          mapa_shared(smem_u32(&acc_empty[1]), 0)};
+        int local = 0;
+        bool ok = true;
+        for (int u = pair_id; u < total_units && ok; u += num_pairs, ++local) {
+            const int grp = u / args.total_tiles;
+            int mt, nt;
+            tile_coords(u - grp * args.total_tiles, args, mt, nt);
+            const long long row = (long long)mt * kPairTileM + rank * 128 + row_local;
+            const int acc = local & 1;
+            const uint32_t acc_phase = (local >> 1) & 1;
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
+            if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
+                ok = false;
+                continue;
+            }
+            tc_fence_after();
+            const uint32_t taddr =
+                tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
+            epilogue_unit<EPI>(args, taddr, row, grp, nt, half);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(empty_remote[acc]);
+        }
+    }
+
+    tc_fence_before();
+    cluster_sync();   // the peer's shared memory is read by the pair's MMAs until here
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem_base, kTmemCols);
+    }
+}
 
 // Scheme II step 4 from the coefficient byte planes [S][Mp][Np] written by the
 // GEMM epilogue: one thread per 4 consecutive columns of a row (a warp reads
@@ -1109,16 +1361,33 @@ static cudaError_t gemm_launch(const CUtensorMap& tmA, const CUtensorMap& tmB, c
     return cudaGetLastError();
 }
 
+template <int EPI>
+static cudaError_t gemm_launch_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
+                                    const GemmArgs& a, int grid, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_gemm_i8_pair<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem);
+    });
+    if (attr != cudaSuccess) return attr;
+    k_gemm_i8_pair<EPI><<<grid, kGemmThreads, kPairSmem, st>>>(tmA, tmB, pairs, a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
+    const int tile_m = p.pair ? kPairTileM : kTileM;
+    if (p.Mp % tile_m != 0) return cudaErrorInvalidValue;
     CUtensorMap tmA, tmB;
-    if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, kTileM)) return cudaErrorInvalidValue;
-    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, kTileN)) return cudaErrorInvalidValue;
+    if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, 128)) return cudaErrorInvalidValue;
+    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, p.pair ? 128 : kTileN))
+        return cudaErrorInvalidValue;
     GemmArgs a{};
-    a.m_tiles = (int)(p.Mp / kTileM);
+    a.m_tiles = (int)(p.Mp / tile_m);
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
     a.total_tiles = a.m_tiles * a.n_tiles;
-    a.band = a.m_tiles < 16 ? a.m_tiles : 16;
+    const int band = p.pair ? 8 : 16;
+    a.band = a.m_tiles < band ? a.m_tiles : band;
     a.groups = p.pairs.num_groups;
     a.Mp = (long long)p.Mp;
     a.Np = (long long)p.Np;
@@ -1126,8 +1395,15 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.ctc = p.ctc;
     a.coef = p.coef;
     a.S = p.planes;
-    if (a.total_tiles == 0 || a.groups == 0) return cudaSuccess;
-    const int grid = a.total_tiles < p.sms ? a.total_tiles : p.sms;
+    const long long units = (long long)a.total_tiles * a.groups;
+    if (units == 0) return cudaSuccess;
+    if (p.pair) {
+        const long long pairs_max = p.sms / 2;
+        const int grid = 2 * (int)(units < pairs_max ? units : pairs_max);
+        return p.coef ? gemm_launch_pair<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
+                      : gemm_launch_pair<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);
+    }
+    const int grid = (int)(units < p.sms ? units : p.sms);
     return p.coef ? gemm_launch<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
                   : gemm_launch<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);
 }

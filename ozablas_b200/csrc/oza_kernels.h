@@ -12,7 +12,8 @@ constexpr int kMaxSlicesHost = 20;
 
 // Tile geometry of the INT8 tensor-core GEMM and the padding it imposes on
 // the workspace layouts.
-constexpr int kTileM = 128;   // rows of A per CTA tile (UMMA M)
+constexpr int kTileM = 128;   // rows of A per CTA tile (UMMA M, one-CTA variant)
+constexpr int kTileMPair = 256;   // rows of A per CTA-pair tile (cta_group::2 variant)
 constexpr int kTileN = 256;   // rows of B^T per CTA tile (UMMA N)
 constexpr int kTileK = 128;   // bytes of K per pipeline stage (one 128B swizzle row)
 
@@ -59,6 +60,7 @@ struct GemmPlan {
     PairList pairs;
     int* err;                 // device error word
     int sms;
+    bool pair;                // cta_group::2 kernel on CTA pairs (Mp multiple of 256)
     // epilogue output: INT32 group planes, or (Scheme II) CRT coefficient bytes
     int32_t* ctc;             // [groups][Mp][Np], used when coef == nullptr
     uint8_t* coef;            // [S][Mp][Np]
