@@ -124,6 +124,26 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
  * OZA_TIMEOUT). */
 oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 
+/* ---- allocation-free GEMM ------------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running while a stream is being captured into a CUDA graph,
+ * code inside an application's own allocator or memory-pool callback, paths
+ * that cannot afford the synchronisation cudaMalloc/cudaFree may imply --
+ * C = A * B by `scheme` with `slices` slices/moduli, with every intermediate
+ * in a fixed device array of OZA_NOALLOC_SCRATCH_BYTES that the library holds
+ * on each GPU it is loaded on until the process exits.  A, B, C as for
+ * oza_gemm (row-major FP64 device buffers on the current device); work is
+ * issued on `stream` (NULL = legacy default stream) and the call returns
+ * asynchronously.  Problems whose intermediates do not fit in the array are
+ * rejected with OZA_UNSUPPORTED and a message giving the bytes needed.  No
+ * cudaMalloc/cudaFree or other allocating call is made.  The first call on a
+ * device looks up the array's device address and uploads the CRT tables, so
+ * make it before any stream capture.  All calls share the one array: calls
+ * whose work overlaps on the GPU race; issue them on one stream. */
+#define OZA_NOALLOC_SCRATCH_BYTES (64u << 20)
+oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
+                              const double* B, double* C, void* stream);
+
 /* ---- host utilities ------------------------------------------------------- */
 /* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from
  * std::mt19937(seed) in row-major order.

@@ -50,6 +50,8 @@ oza_status_t cuda_fail(cudaError_t e, const char* what) {
 
 }  // namespace
 
+void oza::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 struct oza_executor {
     int device = 0;
     int sms = 0;

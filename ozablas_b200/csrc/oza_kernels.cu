@@ -359,7 +359,7 @@ __device__ __forceinline__ int cvt_s8(double v) {
 // symmetric_residue.
 template <int S, bool WIDE, int E>
 __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p, int8_t* dst, size_t plane_stride) {
-    if (!WIDE) {
+    if constexpr (!WIDE) {
         int dlo[E], dhi[E];
 #pragma unroll
         for (int i = 0; i < E; ++i) {
@@ -387,8 +387,7 @@ __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p
             if constexpr (E == 16) *reinterpret_cast<uint4*>(o) = make_uint4(wds[0], wds[1], wds[2], wds[3]);
             else *reinterpret_cast<uint2*>(o) = make_uint2(wds[0], wds[1]);
         }
-        return;
-    }
+    } else {
     int d0[E], d1[E], d2[E], d3[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) {
@@ -407,6 +406,7 @@ __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p
         } else {
             *reinterpret_cast<uint2*>(o) = make_uint2(pack4(r[0], r[1], r[2], r[3]), pack4(r[4], r[5], r[6], r[7]));
         }
+    }
     }
 }
 

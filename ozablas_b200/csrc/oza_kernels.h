@@ -76,4 +76,7 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
                                 const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st);
 
+// Sets the text returned by oza_last_error_string() on this thread.
+void set_last_error(const char* msg);
+
 }  // namespace oza

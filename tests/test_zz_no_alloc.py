@@ -1,0 +1,75 @@
+"""oza_gemm_noalloc: the GEMM for callers that cannot allocate device memory
+(code under stream capture, inside an allocator callback, or on paths that
+cannot afford cudaMalloc's synchronisation).  It keeps every intermediate in
+a fixed device array compiled into the library, so its results must equal
+those of the workspace path (oza_gemm) bit for bit, on consecutive calls
+that reuse the array's leftover contents.  Collected last on purpose."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc():
+    import ozablas_b200 as oz
+    L = oz.lib()
+    fn = L.oza_gemm_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    return oz, L, fn
+
+
+def _setup_call(oz, fn):
+    """The first call on a device looks up the array's address, which makes the
+    driver load the library's module holding the array (the one-time 64 MiB
+    reservation); later calls must not change device memory use."""
+    import torch
+    a = torch.zeros(8, 8, dtype=torch.float64, device="cuda")
+    c = torch.empty(8, 8, dtype=torch.float64, device="cuda")
+    assert fn(2, 4, 8, 8, 8, a.data_ptr(), a.data_ptr(), c.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert bool((c == 0).all())
+
+
+def _run_pair(oz, fn, executor, scheme, S, M, N, K, seeds):
+    import torch
+    A = torch.from_numpy(oz.generate_matrix(M, K, 1.0, seeds[0])).cuda()
+    B = torch.from_numpy(oz.generate_matrix(K, N, 1.0, seeds[1])).cuda()
+    ws = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(executor, M, N, K, S)
+    ref = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    (oz.ozaki_scheme2_gemm if scheme == 2 else oz.ozaki_scheme1_gemm)(ws, A, B, ref)
+    got = torch.full((M, N), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    rc = fn(scheme, S, M, N, K, A.data_ptr(), B.data_ptr(), got.data_ptr(), None)
+    assert rc == 0, oz.lib().oza_last_error_string()
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    return got.view(torch.int64), ref.view(torch.int64), free_before - free_after
+
+
+@pytest.mark.parametrize("scheme,S,shape", [(2, 16, (512, 384, 640)), (2, 8, (100, 70, 333)), (1, 6, (300, 200, 256))])
+def test_noalloc_matches_workspace_path_twice(executor, scheme, S, shape):
+    oz, L, fn = _noalloc()
+    _setup_call(oz, fn)
+    M, N, K = shape
+    # two calls in a row, different inputs: the second reuses the array's contents
+    for seeds in ((42, 43), (7, 8)):
+        got, ref, grown = _run_pair(oz, fn, executor, scheme, S, M, N, K, seeds)
+        assert bool((got == ref).all()), f"seeds {seeds}: results differ from oza_gemm"
+        assert grown == 0, f"device memory in use grew by {grown} bytes during the call"
+
+
+def test_noalloc_rejects_problems_beyond_the_array(executor):
+    import torch
+    oz, L, fn = _noalloc()
+    n = 4096   # 16 moduli: 2 x 256 MiB of residues, far beyond the 64 MiB array
+    A = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    C = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    rc = fn(2, 16, n, n, n, A.data_ptr(), A.data_ptr(), C.data_ptr(), None)
+    assert rc == oz.OZA_UNSUPPORTED
+    assert b"bytes of scratch" in L.oza_last_error_string()
+    assert fn(3, 16, 8, 8, 8, A.data_ptr(), A.data_ptr(), C.data_ptr(), None) == oz.OZA_INVALID_ARG
