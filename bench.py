@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--phi", type=float, default=0.5)
     p.add_argument("--cpu-sample", type=int, default=512, help="rows/cols of the CPU block sample")
     p.add_argument("--no-extras", action="store_true", help="skip DGEMM / reference-GPU / accuracy side numbers")
+    p.add_argument("--suite", default=None, choices=["precision"],
+                   help="precision: precision-targeted rectangular GEMMs with the slice count autotuned to "
+                        "native DGEMM's error (one JSON line per shape and scheme)")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
     return p.parse_args()
@@ -467,8 +470,110 @@ def reference_gpu_tflops(args, dA, dB, stream):
     return 2.0 * M * N * K / (ms * 1e-3) / 1e12
 
 
+# ------------------------------------------------------------------ precision-targeted suite
+PRECISION_SHAPES = [("tall_skinny", 16384, 16384, 1024), ("deep_k", 1024, 1024, 65536)]
+
+
+def precision_inputs(M, N, K, phi=4.0, zero_frac=0.05, seed=42):
+    """phi = 4 inputs with 5% exact zeros and a few rows of A and columns of B
+    (rows and columns of C) scaled by 2^+-300."""
+    import numpy as np
+    import ozablas_b200 as oz
+    A = oz.generate_matrix(M, K, phi, seed)
+    B = oz.generate_matrix(K, N, phi, seed + 1)
+    rng = np.random.default_rng(seed)
+    A[rng.random(A.shape) < zero_frac] = 0.0
+    B[rng.random(B.shape) < zero_frac] = 0.0
+    ra = rng.choice(M, 6, replace=False)
+    cb = rng.choice(N, 6, replace=False)
+    A[ra[:3]] *= 2.0 ** 300
+    A[ra[3:]] *= 2.0 ** -300
+    B[:, cb[:3]] *= 2.0 ** 300
+    B[:, cb[3:]] *= 2.0 ** -300
+    return A, B, sorted(int(i) for i in ra), sorted(int(j) for j in cb)
+
+
+def run_precision_suite(args, local):
+    """Per shape: native DGEMM's sampled error vs a double-double reference is
+    the target; the autotuner picks the smallest slice count meeting it on a
+    seeded block; the full GEMM then runs at that count and its error is
+    checked on a second, independent block (and on the scaled rows)."""
+    import numpy as np
+    import torch
+    import ozablas_b200 as oz
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ex = oz.CudaExecutor(local)
+    stream = torch.cuda.current_stream(dev)
+    ex.set_stream(stream.cuda_stream)
+    block, tune_seed, val_seed = 256, 1, 2
+    for name, M, N, K in PRECISION_SHAPES:
+        hA, hB, ra, cb = precision_inputs(M, N, K)
+        dA = torch.from_numpy(hA).to(dev)
+        dB = torch.from_numpy(hB).to(dev)
+        dD = torch.empty(M, N, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            torch.matmul(dA, dB, out=dD)
+        dms = time_events(lambda: torch.matmul(dA, dB, out=dD), 5, stream)
+        target = oz.block_error(ex, dA, dB, dD, M, N, K, block, tune_seed)
+        dgemm_val = oz.block_error(ex, dA, dB, dD, M, N, K, block, val_seed)
+        flops = 2.0 * M * N * K
+        for scheme in (2, 1):
+            t0 = time.perf_counter()
+            try:
+                S, tuned = oz.autotune_slices(ex, scheme, dA, dB, M, N, K, target, block, tune_seed)
+                met = True
+            except oz.OzaError as e:
+                S, tuned, met = 20, float("nan"), False
+                note = str(e)
+            tune_s = time.perf_counter() - t0
+            W = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(ex, M, N, K, S)
+            gemm = oz.ozaki_scheme2_gemm if scheme == 2 else oz.ozaki_scheme1_gemm
+            dC = torch.empty(M, N, dtype=torch.float64, device=dev)
+            for _ in range(args.warmup):
+                gemm(W, dA, dB, dC)
+            with ClockSampler(local) as clk:
+                ms = time_events(lambda: gemm(W, dA, dB, dC), args.steps, stream)
+            val = oz.block_error(ex, dA, dB, dC, M, N, K, block, val_seed)
+            # the scaled rows and columns of C, against DGEMM on the same entries
+            sub = torch.tensor(ra, device=dev)
+            subc = torch.tensor(cb, device=dev)
+            Ar = dA.index_select(0, sub).contiguous()
+            Bc = dB.index_select(1, subc).contiguous()
+            Cr = dC.index_select(0, sub).index_select(1, subc).contiguous()
+            Dr = dD.index_select(0, sub).index_select(1, subc).contiguous()
+            scaled = oz.block_error(ex, Ar, Bc, Cr, len(ra), len(cb), K, 64, 0)
+            scaled_d = oz.block_error(ex, Ar, Bc, Dr, len(ra), len(cb), K, 64, 0)
+            line = {
+                "suite": "precision", "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT,
+                "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "config": {"workload": f"precision_{name}_{M}x{N}x{K}", "M": M, "N": N, "K": K,
+                           "scheme": scheme, "phi": 4.0, "zeros": 0.05,
+                           "scaled": "3 rows of A and 3 columns of B by 2^300, 3 each by 2^-300",
+                           "input_seed": 42},
+                "slices": S, "target_met_on_tuning_block": met,
+                "target_rel_err": target, "tuned_block_err": tuned,
+                "validation_err": val, "cublas_dgemm_validation_err": dgemm_val,
+                "scaled_entries_err": scaled, "cublas_dgemm_scaled_entries_err": scaled_d,
+                "error_reference": f"double-double GPU GEMM on {block}x{block} seeded row/column blocks",
+                "autotune_s": tune_s, "cublas_dgemm_tflops": flops / (dms * 1e-3) / 1e12,
+                "clocks": clk.summary(),
+            }
+            if not met:
+                line["note"] = note
+            print(json.dumps(line), flush=True)
+            del W, dC
+            torch.cuda.empty_cache()
+        del dA, dB, dD
+        torch.cuda.empty_cache()
+
+
 def main():
     args = parse()
+    if args.suite == "precision":
+        run_precision_suite(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     ws, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -144,6 +144,25 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
 
+/* ---- accuracy tools ------------------------------------------------------- */
+/* Maximum relative error of C (M x N, device) against a double-double
+ * reference of the same entries, over a seeded sample of `block` rows x `block`
+ * columns (relative error falls back to absolute where the reference is 0).
+ * Extension: the reference measures accuracy with its FP128 CPU oracle and
+ * compute_errors (utils/matrix_reference.hpp:22-50, utils/matrix_compare.hpp:24-65). */
+oza_status_t oza_block_error(oza_exec_t ex, const double* A, const double* B, const double* C, size_t M, size_t N,
+                             size_t K, int block, unsigned seed, double* max_rel_err);
+
+/* Accuracy-target knob: the smallest slice count (1..20) whose result meets
+ * `target_rel_err` on a seeded block sample of this A and B (the pipeline run
+ * on the gathered rows and columns reproduces those entries of the full run
+ * exactly).  Returns OZA_UNSUPPORTED with slices = 20 if even 20 misses.
+ * Extension: the reference leaves the choice of `slices` to the caller
+ * (its precision benchmarks sweep it, precision_benchmarks/02_...:146-178). */
+oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, const double* A,
+                                 const double* B, double target_rel_err, int block, unsigned seed, int* slices,
+                                 double* achieved_err);
+
 /* ---- host utilities ------------------------------------------------------- */
 /* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from
  * std::mt19937(seed) in row-major order.

@@ -25,7 +25,8 @@ from dataclasses import dataclass
 __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
-    "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols",
+    "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
+    "autotune_slices",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -102,6 +103,9 @@ def lib() -> ctypes.CDLL:
         "oza_ws_device_error": (I, [P, ctypes.POINTER(I)]),
         "oza_generate_matrix": (I, [I, I, ctypes.c_double, I, P]),
         "oza_scheme1_beta": (I, [S]),
+        "oza_block_error": (I, [P, P, P, P, S, S, S, I, U, ctypes.POINTER(ctypes.c_double)]),
+        "oza_autotune_slices": (I, [P, I, S, S, S, P, P, ctypes.c_double, I, U, ctypes.POINTER(I),
+                                    ctypes.POINTER(ctypes.c_double)]),
         "oza_scheme2_k_param": (I, [I, S]),
     }
     for name, (res, args) in sig.items():
@@ -309,6 +313,28 @@ def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):
     _check(lib().oza_generate_matrix(int(rows), int(cols), float(phi), int(seed),
                                      out.ctypes.data_as(ctypes.c_void_p)))
     return out
+
+
+def block_error(executor, A, B, C, M: int, N: int, K: int, block: int = 96, seed: int = 7) -> float:
+    """Max relative error of C against a double-double reference on a seeded
+    block of `block` rows x `block` columns (device matrices)."""
+    e = ctypes.c_double()
+    _check(lib().oza_block_error(executor.handle, ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)),
+                                 ctypes.c_void_p(_ptr(C)), int(M), int(N), int(K), int(block), int(seed),
+                                 ctypes.byref(e)))
+    return e.value
+
+
+def autotune_slices(executor, scheme: int, A, B, M: int, N: int, K: int, target_rel_err: float,
+                    block: int = 96, seed: int = 7):
+    """Smallest slice count meeting target_rel_err on a sampled block; returns
+    (slices, sampled error).  Raises OzaError if 20 slices miss the target."""
+    s = ctypes.c_int()
+    e = ctypes.c_double()
+    _check(lib().oza_autotune_slices(executor.handle, int(scheme), int(M), int(N), int(K),
+                                     ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)), float(target_rel_err),
+                                     int(block), int(seed), ctypes.byref(s), ctypes.byref(e)))
+    return s.value, e.value
 
 
 def scheme1_beta(K: int) -> int:

@@ -1,0 +1,200 @@
+// oza_tune_host.cpp -- C ABI of the accuracy tools (see oza_tune.cu):
+// oza_block_error and oza_autotune_slices.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "oza_capi.h"
+#include "oza_kernels.h"
+
+namespace oza {
+cudaError_t launch_dd_block_gemm(const double* A, const double* B, int r, int c, size_t K, double* C,
+                                 cudaStream_t st);
+cudaError_t launch_gather_block(const double* A, const double* B, size_t M, size_t N, size_t K,
+                                const long long* rows, int r, const long long* cols, int c, double* Ab, double* Bb,
+                                cudaStream_t st);
+}  // namespace oza
+
+namespace {
+
+oza_status_t tfail(oza_status_t st, const std::string& m) {
+    oza::set_last_error(m.c_str());
+    return st;
+}
+
+std::vector<long long> sample_indices(size_t n, int k, std::mt19937_64& rng) {
+    std::vector<long long> idx;
+    if ((size_t)k >= n) {
+        idx.resize(n);
+        std::iota(idx.begin(), idx.end(), 0ll);
+        return idx;
+    }
+    std::vector<long long> all(n);
+    std::iota(all.begin(), all.end(), 0ll);
+    for (int i = 0; i < k; ++i) {   // partial Fisher-Yates
+        std::uniform_int_distribution<size_t> d(i, n - 1);
+        std::swap(all[i], all[d(rng)]);
+    }
+    idx.assign(all.begin(), all.begin() + k);
+    std::sort(idx.begin(), idx.end());
+    return idx;
+}
+
+// Max relative error of got against ref (absolute where ref is 0), as
+// utils/matrix_compare.hpp:24-65 of the reference measures it.
+double max_rel(const std::vector<double>& got, const std::vector<double>& ref) {
+    double m = 0.0;
+    for (size_t i = 0; i < ref.size(); ++i) {
+        const double d = std::fabs(got[i] - ref[i]);
+        const double r = ref[i] != 0.0 ? d / std::fabs(ref[i]) : d;
+        if (!(r <= m)) m = r;   // NaN propagates as the maximum
+    }
+    return m;
+}
+
+// Device buffers of one sampled block and its double-double reference.
+struct Block {
+    oza_exec_t ex = nullptr;
+    int r = 0, c = 0;
+    size_t K = 0;
+    std::vector<long long> rows, cols;
+    void* d_idx = nullptr;
+    double* Ab = nullptr;
+    double* Bb = nullptr;
+    double* Cb = nullptr;
+    double* Rb = nullptr;
+    std::vector<double> ref;
+    ~Block() {
+        void* bufs[] = {d_idx, Ab, Bb, Cb, Rb};
+        for (void* p : bufs)
+            if (p) oza_executor_free(ex, p);
+    }
+};
+
+oza_status_t make_block(oza_exec_t ex, const double* A, const double* B, size_t M, size_t N, size_t K, int block,
+                        unsigned seed, Block& b) {
+    if (block < 1) return tfail(OZA_INVALID_ARG, "block size must be >= 1");
+    std::mt19937_64 rng(seed);
+    b.ex = ex;
+    b.K = K;
+    b.rows = sample_indices(M, block, rng);
+    b.cols = sample_indices(N, block, rng);
+    b.r = (int)b.rows.size();
+    b.c = (int)b.cols.size();
+    const size_t nidx = b.rows.size() + b.cols.size();
+    oza_status_t st;
+    if ((st = oza_executor_alloc(ex, &b.d_idx, nidx * sizeof(long long))) != OZA_OK) return st;
+    if ((st = oza_executor_alloc(ex, (void**)&b.Ab, (size_t)b.r * K * sizeof(double) + 8)) != OZA_OK) return st;
+    if ((st = oza_executor_alloc(ex, (void**)&b.Bb, K * (size_t)b.c * sizeof(double) + 8)) != OZA_OK) return st;
+    if ((st = oza_executor_alloc(ex, (void**)&b.Cb, (size_t)b.r * b.c * sizeof(double))) != OZA_OK) return st;
+    if ((st = oza_executor_alloc(ex, (void**)&b.Rb, (size_t)b.r * b.c * sizeof(double))) != OZA_OK) return st;
+    std::vector<long long> idx(b.rows);
+    idx.insert(idx.end(), b.cols.begin(), b.cols.end());
+    if ((st = oza_executor_copy(ex, b.d_idx, idx.data(), nidx * sizeof(long long), 1)) != OZA_OK) return st;
+    const long long* drows = static_cast<const long long*>(b.d_idx);
+    int dev = 0, prev = -1;
+    if ((st = oza_executor_device(ex, &dev)) != OZA_OK) return st;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return tfail(OZA_CUDA_ERROR, "cudaSetDevice failed");
+    cudaError_t e = oza::launch_gather_block(A, B, M, N, K, drows, b.r, drows + b.r, b.c, b.Ab, b.Bb, nullptr);
+    if (e == cudaSuccess) e = oza::launch_dd_block_gemm(b.Ab, b.Bb, b.r, b.c, K, b.Rb, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    if (e != cudaSuccess) return tfail(OZA_CUDA_ERROR, std::string("sampled reference: ") + cudaGetErrorString(e));
+    b.ref.resize((size_t)b.r * b.c);
+    return oza_executor_copy(ex, b.ref.data(), b.Rb, b.ref.size() * sizeof(double), 2);
+}
+
+// Ozaki result on the block for one scheme / slice count, and its error.
+oza_status_t block_trial(Block& b, int scheme, int slices, double* err) {
+    oza_ws_t ws = nullptr;
+    oza_status_t st = oza_ws_create(b.ex, scheme, (size_t)b.r, (size_t)b.c, b.K, slices, 0u, &ws);
+    if (st != OZA_OK) return st;
+    oza_timings_t t;   // synchronous
+    st = oza_gemm(ws, b.Ab, b.Bb, b.Cb, &t);
+    oza_ws_destroy(ws);
+    if (st != OZA_OK) return st;
+    std::vector<double> got(b.ref.size());
+    st = oza_executor_copy(b.ex, got.data(), b.Cb, got.size() * sizeof(double), 2);
+    if (st != OZA_OK) return st;
+    *err = max_rel(got, b.ref);
+    return OZA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+oza_status_t oza_block_error(oza_exec_t ex, const double* A, const double* B, const double* C, size_t M, size_t N,
+                             size_t K, int block, unsigned seed, double* max_rel_err) {
+    if (!ex || !A || !B || !C || !max_rel_err) return tfail(OZA_INVALID_ARG, "oza_block_error: null argument");
+    if (M == 0 || N == 0) {
+        *max_rel_err = 0.0;
+        return OZA_OK;
+    }
+    Block b;
+    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
+    if (st != OZA_OK) return st;
+    std::vector<double> got((size_t)b.r * b.c);
+    for (int i = 0; i < b.r; ++i) {
+        std::vector<double> row(N);
+        st = oza_executor_copy(ex, row.data(), C + (size_t)b.rows[i] * N, N * sizeof(double), 2);
+        if (st != OZA_OK) return st;
+        for (int j = 0; j < b.c; ++j) got[(size_t)i * b.c + j] = row[b.cols[j]];
+    }
+    *max_rel_err = max_rel(got, b.ref);
+    return OZA_OK;
+}
+
+oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, const double* A,
+                                 const double* B, double target_rel_err, int block, unsigned seed, int* slices,
+                                 double* achieved_err) {
+    if (!ex || !A || !B || !slices) return tfail(OZA_INVALID_ARG, "oza_autotune_slices: null argument");
+    if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return tfail(OZA_INVALID_ARG, "oza_autotune_slices: scheme");
+    if (!(target_rel_err > 0.0)) return tfail(OZA_INVALID_ARG, "oza_autotune_slices: target must be > 0");
+    if (M == 0 || N == 0 || K == 0) {
+        *slices = 1;
+        if (achieved_err) *achieved_err = 0.0;
+        return OZA_OK;
+    }
+    Block b;
+    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
+    if (st != OZA_OK) return st;
+    // Smallest S in [1, 20] meeting the target, by bisection on the
+    // (monotonically falling) sampled error, then a check one below.
+    int lo = 1, hi = 20;
+    double err_hi = 0.0;
+    if ((st = block_trial(b, scheme, hi, &err_hi)) != OZA_OK) return st;
+    if (!(err_hi <= target_rel_err)) {
+        *slices = hi;
+        if (achieved_err) *achieved_err = err_hi;
+        char m[160];
+        snprintf(m, sizeof(m), "oza_autotune_slices: target %.3g not reached with 20 slices (sampled error %.3g)",
+                 target_rel_err, err_hi);
+        return tfail(OZA_UNSUPPORTED, m);
+    }
+    double best_err = err_hi;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        double e = 0.0;
+        if ((st = block_trial(b, scheme, mid, &e)) != OZA_OK) return st;
+        if (e <= target_rel_err) {
+            hi = mid;
+            best_err = e;
+        } else {
+            lo = mid + 1;
+        }
+    }
+    if (hi == 20) best_err = err_hi;
+    *slices = hi;
+    if (achieved_err) *achieved_err = best_err;
+    return OZA_OK;
+}
+
+}  // extern "C"

@@ -106,3 +106,14 @@ int main() {
                     f"-L{root}/ozablas_b200", "-loza_b200", f"-Wl,-rpath,{root}/ozablas_b200"], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
     assert "sm_100a" in out and "hip rejected" in out
+
+
+def test_accuracy_tools_reject_null_arguments():
+    """oza_block_error / oza_autotune_slices validate their arguments before
+    touching a device."""
+    L = oz.lib()
+    s, e = ctypes.c_int(), ctypes.c_double()
+    assert L.oza_autotune_slices(None, 2, 4, 4, 4, None, None, 1e-10, 8, 0, ctypes.byref(s),
+                                 ctypes.byref(e)) == oz.OZA_INVALID_ARG
+    assert L.oza_block_error(None, None, None, None, 4, 4, 4, 8, 0, ctypes.byref(e)) == oz.OZA_INVALID_ARG
+    assert "null" in L.oza_last_error_string().decode()
