@@ -144,6 +144,39 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
 
+/* ---- grouped Scheme II GEMM ------------------------------------------------ */
+/* Many independent row-major FP64 GEMMs C_i = A_i (M_i x K_i) * B_i (K_i x N_i),
+ * each with its own slice count, run as one launch per stage: step 1 and 2
+ * over all problems, one persistent tcgen05 GEMM over every problem's work
+ * units, one CRT launch (stages 2 and 4 once per distinct slice count).  The
+ * sequence is captured into a CUDA graph on the first call and replayed.
+ * Results are bit-identical to oza_gemm on each problem alone.
+ * Extension: the reference runs one GEMM per call (include/ozablas/ozablas.hpp:31). */
+typedef struct oza_group* oza_group_t;
+
+#define OZA_GROUP_NO_GRAPH 0x2u /* launch the stages directly instead of replaying a graph */
+
+typedef struct {
+    size_t count;  /* problems */
+    size_t units;  /* GEMM work units (problem, m-tile, n-tile, modulus) */
+    size_t bytes;  /* device memory held */
+    int launches;  /* kernel launches per call */
+    int graph;     /* 1 if calls replay a CUDA graph */
+} oza_group_info_t;
+
+/* M, N, K, slices: arrays of `count` entries; every dimension >= 1, slices
+ * 1..20.  Only Scheme II is grouped (OZA_UNSUPPORTED otherwise). */
+oza_status_t oza_group_create(oza_exec_t ex, int scheme, size_t count, const size_t* M, const size_t* N,
+                              const size_t* K, const int* slices, unsigned flags, oza_group_t* out);
+oza_status_t oza_group_destroy(oza_group_t g);
+/* A, B, C: host arrays of `count` device pointers.  Asynchronous on the
+ * executor's stream unless timings is non-null (then the stages run without
+ * the graph, bracketed by events, and the call synchronises). */
+oza_status_t oza_group_gemm(oza_group_t g, const double* const* A, const double* const* B, double* const* C,
+                            oza_timings_t* timings);
+oza_status_t oza_group_get_info(oza_group_t g, oza_group_info_t* info);
+oza_status_t oza_group_device_error(oza_group_t g, int* code);
+
 /* ---- accuracy tools ------------------------------------------------------- */
 /* Maximum relative error of C (M x N, device) against a double-double
  * reference of the same entries, over a seeded sample of `block` rows x `block`

@@ -26,7 +26,7 @@ __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
-    "autotune_slices",
+    "autotune_slices", "GroupGemm",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -36,6 +36,7 @@ HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "oza_capi.h")
 OZA_OK, OZA_INVALID_ARG, OZA_OOM, OZA_CUDA_ERROR, OZA_TIMEOUT, OZA_UNSUPPORTED = range(6)
 OZA_SCHEME1, OZA_SCHEME2 = 1, 2
 OZA_WS_MATERIALIZE = 0x1
+OZA_GROUP_NO_GRAPH = 0x2
 BUF_SHIFT_A, BUF_SHIFT_B, BUF_A_SLICES, BUF_B_SLICES, BUF_C_TC = range(5)
 
 
@@ -58,6 +59,11 @@ class _WsInfo(ctypes.Structure):
                 ("Mp", ctypes.c_size_t), ("Np", ctypes.c_size_t), ("Kp", ctypes.c_size_t),
                 ("groups", ctypes.c_int), ("k_param", ctypes.c_int), ("beta", ctypes.c_int),
                 ("flags", ctypes.c_uint), ("bytes", ctypes.c_size_t)]
+
+
+class _GroupInfo(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_size_t), ("units", ctypes.c_size_t), ("bytes", ctypes.c_size_t),
+                ("launches", ctypes.c_int), ("graph", ctypes.c_int)]
 
 
 @dataclass
@@ -107,6 +113,13 @@ def lib() -> ctypes.CDLL:
         "oza_autotune_slices": (I, [P, I, S, S, S, P, P, ctypes.c_double, I, U, ctypes.POINTER(I),
                                     ctypes.POINTER(ctypes.c_double)]),
         "oza_scheme2_k_param": (I, [I, S]),
+        "oza_group_create": (I, [P, I, S, ctypes.POINTER(S), ctypes.POINTER(S), ctypes.POINTER(S),
+                                 ctypes.POINTER(I), U, ctypes.POINTER(P)]),
+        "oza_group_destroy": (I, [P]),
+        "oza_group_gemm": (I, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P),
+                               ctypes.POINTER(_Timings)]),
+        "oza_group_get_info": (I, [P, ctypes.POINTER(_GroupInfo)]),
+        "oza_group_device_error": (I, [P, ctypes.POINTER(I)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -303,6 +316,68 @@ def ozaki_scheme2_gemm(ws: WorkspaceScheme2, A, B, C, timings: OzaTimings | None
         raise TypeError("ozaki_scheme2_gemm needs a WorkspaceScheme2")
     _check_shapes(ws, A, B, C)
     _gemm(ws, A, B, C, timings)
+
+
+class GroupGemm:
+    """Many independent Scheme II FP64 GEMMs of different shapes, run as one
+    launch per stage and replayed from a CUDA graph (extension; the reference
+    runs one GEMM per call).
+
+        g = GroupGemm(ex, [(M0, N0, K0), (M1, N1, K1), ...], slices=16)
+        g(As, Bs, Cs)     # lists of device matrices, asynchronous
+    """
+
+    def __init__(self, executor, shapes, slices, graph: bool = True):
+        if not isinstance(executor, CudaExecutor):
+            raise OzaError("OzaBLAS: No suitable hardware backend found for the provided Executor.")
+        self._exec = executor
+        shapes = [tuple(int(x) for x in s) for s in shapes]
+        n = len(shapes)
+        if isinstance(slices, int):
+            slices = [slices] * n
+        if len(slices) != n:
+            raise ValueError("one slice count per problem")
+        self.shapes = shapes
+        self.slices = [int(s) for s in slices]
+        arr = ctypes.c_size_t * n
+        Ms, Ns, Ks = arr(*[s[0] for s in shapes]), arr(*[s[1] for s in shapes]), arr(*[s[2] for s in shapes])
+        Ss = (ctypes.c_int * n)(*self.slices)
+        h = ctypes.c_void_p()
+        _check(lib().oza_group_create(executor.handle, OZA_SCHEME2, n, Ms, Ns, Ks, Ss,
+                                      0 if graph else OZA_GROUP_NO_GRAPH, ctypes.byref(h)))
+        self._h = h
+        info = _GroupInfo()
+        _check(lib().oza_group_get_info(h, ctypes.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in _GroupInfo._fields_}
+        self._parr = ctypes.c_void_p * n
+
+    def __call__(self, As, Bs, Cs, timings: OzaTimings | None = None) -> None:
+        n = len(self.shapes)
+        if not (len(As) == len(Bs) == len(Cs) == n):
+            raise ValueError(f"expected {n} matrices of each operand")
+        for (M, N, K), A, B, C in zip(self.shapes, As, Bs, Cs):
+            if hasattr(A, "shape") and (tuple(A.shape) != (M, K) or tuple(B.shape) != (K, N)
+                                        or tuple(C.shape) != (M, N)):
+                raise ValueError(f"shapes do not match problem {(M, N, K)}")
+        pa = self._parr(*[_ptr(a) for a in As])
+        pb = self._parr(*[_ptr(b) for b in Bs])
+        pc = self._parr(*[_ptr(c) for c in Cs])
+        t = _Timings() if timings is not None else None
+        _check(lib().oza_group_gemm(self._h, pa, pb, pc, ctypes.byref(t) if t is not None else None))
+        if timings is not None:
+            for f, _ in _Timings._fields_:
+                setattr(timings, f, float(getattr(t, f)))
+
+    def device_error(self) -> int:
+        c = ctypes.c_int()
+        _check(lib().oza_group_device_error(self._h, ctypes.byref(c)))
+        return c.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.oza_group_destroy(h)
+            self._h = None
 
 
 def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):

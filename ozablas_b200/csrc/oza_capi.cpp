@@ -18,7 +18,10 @@
 #include <string>
 
 #include "oza_capi.h"
+#include "oza_internal.h"
 #include "oza_kernels.h"
+
+using oza::DeviceGuard;
 
 namespace {
 
@@ -52,13 +55,6 @@ oza_status_t cuda_fail(cudaError_t e, const char* what) {
 
 void oza::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
-struct oza_executor {
-    int device = 0;
-    int sms = 0;
-    cudaStream_t stream = nullptr;   // legacy default stream unless set
-    void* blas = nullptr;            // cuBLAS handle created on first request
-    std::mutex blas_mu;
-};
 
 struct oza_workspace {
     oza_executor* ex = nullptr;
@@ -83,19 +79,6 @@ struct oza_workspace {
 
 namespace {
 
-// Make the executor's device current for the duration of a call.
-struct DeviceGuard {
-    int prev = -1;
-    bool ok = true;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 void ws_release(oza_workspace* ws) {
     void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->coef, ws->err};

@@ -21,7 +21,13 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <memory>
 #include <mutex>
+#include <new>
+#include <utility>
+#include <vector>
 
 #include "oza_device.cuh"
 #include "oza_kernels.h"
@@ -204,6 +210,32 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
     return v;
 }
 
+// Maximum magnitude bit pattern of one row (one warp, all lanes get it).
+__device__ __forceinline__ unsigned long long row_max_bits(const double* row, long long cols, int lane, bool vec2) {
+    unsigned long long mx = 0;
+    if (vec2) {
+        const double2* row2 = reinterpret_cast<const double2*>(row);
+        long long n2 = cols >> 1;
+        for (long long k = lane; k < n2; k += 32) {
+            double2 v = __ldg(row2 + k);
+            unsigned long long a = (unsigned long long)__double_as_longlong(v.x) & kMagMask;
+            unsigned long long b = (unsigned long long)__double_as_longlong(v.y) & kMagMask;
+            mx = a > mx ? a : mx;
+            mx = b > mx ? b : mx;
+        }
+        if ((cols & 1) && lane == 0) {
+            unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + cols - 1)) & kMagMask;
+            mx = a > mx ? a : mx;
+        }
+    } else {
+        for (long long k = lane; k < cols; k += 32) {
+            unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + k)) & kMagMask;
+            mx = a > mx ? a : mx;
+        }
+    }
+    return warp_max_u64(mx);
+}
+
 // One warp per row of A: shift[r] = offset - max frexp exponent (-1023 for an
 // all-zero row).  Reference: compute_row_shifts_A, step1_statistics.hpp:23-76.
 // The maximum exponent is taken from the maximum magnitude bit pattern, which
@@ -214,44 +246,24 @@ __global__ void __launch_bounds__(256) k_stats_rows(const double* __restrict__ A
     const long long warps_total = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
          r += warps_total) {
-        const double* row = A + r * cols;
-        unsigned long long mx = 0;
-        if (vec2) {
-            const double2* row2 = reinterpret_cast<const double2*>(row);
-            long long n2 = cols >> 1;
-            for (long long k = lane; k < n2; k += 32) {
-                double2 v = __ldg(row2 + k);
-                unsigned long long a = (unsigned long long)__double_as_longlong(v.x) & kMagMask;
-                unsigned long long b = (unsigned long long)__double_as_longlong(v.y) & kMagMask;
-                mx = a > mx ? a : mx;
-                mx = b > mx ? b : mx;
-            }
-            if ((cols & 1) && lane == 0) {
-                unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + cols - 1)) & kMagMask;
-                mx = a > mx ? a : mx;
-            }
-        } else {
-            for (long long k = lane; k < cols; k += 32) {
-                unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + k)) & kMagMask;
-                mx = a > mx ? a : mx;
-            }
-        }
-        mx = warp_max_u64(mx);
+        const unsigned long long mx = row_max_bits(A + r * cols, cols, lane, vec2);
         if (lane == 0) shift[r] = offset - max_exp_from_bits(mx);
     }
 }
 
 // Column maxima of B (K x N) as magnitude bits, combined with atomicMax into
 // colmax[] (zeroed beforehand; 0 encodes an all-zero column).  Block: 8 warps
-// over a 64-column strip, each lane owning 2 adjacent columns; grid.y splits
-// the rows.  Reference: compute_col_shifts_B, step1_statistics.hpp:78-99.
-__global__ void __launch_bounds__(256) k_stats_cols(const double* __restrict__ B, long long rows, long long cols,
-                                                    unsigned long long* __restrict__ colmax) {
+// over the 64-column strip `strip`, each lane owning 2 adjacent columns; the
+// block visits rows y0*8 + warp + i*ystride*8.  Reference:
+// compute_col_shifts_B, step1_statistics.hpp:78-99.
+__device__ __forceinline__ void stats_cols_block(const double* __restrict__ B, long long rows, long long cols,
+                                                 unsigned long long* __restrict__ colmax, long long strip,
+                                                 long long y0, long long ystride) {
     __shared__ unsigned long long part[8][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long c0 = (long long)blockIdx.x * 64 + 2 * lane;
+    const long long c0 = strip * 64 + 2 * lane;
     unsigned long long m0 = 0, m1 = 0;
-    for (long long r = (long long)blockIdx.y * 8 + warp; r < rows; r += (long long)gridDim.y * 8) {
+    for (long long r = y0 * 8 + warp; r < rows; r += ystride * 8) {
         const double* row = B + r * cols;
         if (c0 < cols) {
             unsigned long long a = (unsigned long long)__double_as_longlong(__ldg(row + c0)) & kMagMask;
@@ -269,9 +281,14 @@ __global__ void __launch_bounds__(256) k_stats_cols(const double* __restrict__ B
         unsigned long long m = 0;
 #pragma unroll
         for (int w = 0; w < 8; ++w) m = part[w][threadIdx.x] > m ? part[w][threadIdx.x] : m;
-        long long c = (long long)blockIdx.x * 64 + threadIdx.x;
+        long long c = strip * 64 + threadIdx.x;
         if (c < cols && m != 0) atomicMax(colmax + c, m);
     }
+}
+
+__global__ void __launch_bounds__(256) k_stats_cols(const double* __restrict__ B, long long rows, long long cols,
+                                                    unsigned long long* __restrict__ colmax) {
+    stats_cols_block(B, rows, cols, colmax, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -442,51 +459,61 @@ __device__ __forceinline__ void slices16(const double (&vin)[16], int e, int bet
 // A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per E
 // consecutive columns of a row (E = 8 for Scheme II, 8-byte stores per plane;
 // 16 for Scheme I), coalesced.  Scheme II is instantiated per slice count SC
-// (= S); Scheme I takes S at run time.
+// (= S); Scheme I takes S at run time.  `id` is the chunk index over the
+// padded rows_p x (cols_p / E) chunks.
+template <int SCHEME, int SC, bool WIDE>
+__device__ __forceinline__ void slice_rows_chunk(const double* __restrict__ A, long long rows, long long cols,
+                                                 const int32_t* __restrict__ shift, int S, int beta,
+                                                 int8_t* __restrict__ out, long long cols_p, size_t plane,
+                                                 long long id) {
+    constexpr int E = SCHEME == 2 ? 8 : 16;
+    const long long chunks_per_row = cols_p / E;
+    const long long r = id / chunks_per_row;
+    const long long c0 = (id - r * chunks_per_row) * E;
+    double v[E];
+    int sh = 0;
+    if (r < rows) {
+        sh = shift[r];
+        const double* src = A + r * cols + c0;
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
+    } else {
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = 0.0;
+    }
+    int8_t* dst = out + (size_t)r * cols_p + c0;
+    if (SCHEME == 2) {
+        residuesE<SC, WIDE, E>(v, sh, pow2_or_zero(sh), dst, plane);
+    } else {
+        slices16(reinterpret_cast<const double(&)[16]>(v), r < rows ? -sh : -1023, beta, S,
+                 reinterpret_cast<uint4*>(dst), plane);
+    }
+}
+
 template <int SCHEME, int SC, bool WIDE>
 __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_rows(
     const double* __restrict__ A, long long rows, long long cols, const int32_t* __restrict__ shift, int S, int beta,
     int8_t* __restrict__ out, long long rows_p, long long cols_p) {
     constexpr int E = SCHEME == 2 ? 8 : 16;
-    const long long chunks_per_row = cols_p / E;
-    const long long total = rows_p * chunks_per_row;
+    const long long total = rows_p * (cols_p / E);
     const size_t plane = (size_t)rows_p * (size_t)cols_p;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x) {
-        const long long r = id / chunks_per_row;
-        const long long c0 = (id - r * chunks_per_row) * E;
-        double v[E];
-        int sh = 0;
-        if (r < rows) {
-            sh = shift[r];
-            const double* src = A + r * cols + c0;
-#pragma unroll
-            for (int i = 0; i < E; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
-        } else {
-#pragma unroll
-            for (int i = 0; i < E; ++i) v[i] = 0.0;
-        }
-        int8_t* dst = out + (size_t)r * cols_p + c0;
-        if (SCHEME == 2) {
-            residuesE<SC, WIDE, E>(v, sh, pow2_or_zero(sh), dst, plane);
-        } else {
-            slices16(reinterpret_cast<const double(&)[16]>(v), r < rows ? -sh : -1023, beta, S,
-                     reinterpret_cast<uint4*>(dst), plane);
-        }
-    }
+         id += (long long)gridDim.x * blockDim.x)
+        slice_rows_chunk<SCHEME, SC, WIDE>(A, rows, cols, shift, S, beta, out, cols_p, plane, id);
 }
 
-// B (K x N, row-major) -> out[s][Np][Kp], i.e. B^T, K-major.  Tile of 128 k x
-// 32 n staged through shared memory; thread (n, kg) emits 16 consecutive k of
-// column n.  Also writes shift[n] = offset - max exponent of column n.
+// B (K x N, row-major) -> out[s][Np][Kp], i.e. B^T, K-major.  Tile (bx, by) of
+// 128 k x 32 n staged through shared memory; thread (n, kg) emits 16
+// consecutive k of column n.  Also writes shift[n] = offset - max exponent of
+// column n.
 template <int SCHEME, int SC, bool WIDE>
-__global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const double* __restrict__ B, long long K, long long N,
-                                                    const unsigned long long* __restrict__ colmax, int offset,
-                                                    int S, int beta, int32_t* __restrict__ shift,
-                                                    int8_t* __restrict__ out, long long Np, long long Kp) {
+__device__ __forceinline__ void slice_cols_tile(const double* __restrict__ B, long long K, long long N,
+                                                const unsigned long long* __restrict__ colmax, int offset, int S,
+                                                int beta, int32_t* __restrict__ shift, int8_t* __restrict__ out,
+                                                long long Np, long long Kp, long long bx, long long by) {
     __shared__ double tile[128][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long n0 = (long long)blockIdx.x * 32, k0 = (long long)blockIdx.y * 128;
+    const long long n0 = bx * 32, k0 = by * 128;
     // Load: warp w reads rows k0 + w + 8 i, 32 consecutive columns.
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
@@ -498,7 +525,7 @@ __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const
     const int kg = warp;   // 16-row group
     int e = (n < N) ? max_exp_from_bits(colmax[n]) : -1023;
     int sh = offset - e;
-    if (blockIdx.y == 0 && kg == 0 && n < N) shift[n] = sh;
+    if (by == 0 && kg == 0 && n < N) shift[n] = sh;
     double v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = tile[kg * 16 + i][lane];
@@ -509,6 +536,14 @@ __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const
     } else {
         slices16(v, e, beta, S, reinterpret_cast<uint4*>(dst), plane);
     }
+}
+
+template <int SCHEME, int SC, bool WIDE>
+__global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const double* __restrict__ B, long long K, long long N,
+                                                    const unsigned long long* __restrict__ colmax, int offset,
+                                                    int S, int beta, int32_t* __restrict__ shift,
+                                                    int8_t* __restrict__ out, long long Np, long long Kp) {
+    slice_cols_tile<SCHEME, SC, WIDE>(B, K, N, colmax, offset, S, beta, shift, out, Np, Kp, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -702,10 +737,10 @@ __device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, i
 // One work unit's epilogue for one warp: 32 TMEM lanes (rows) x 128 columns
 // (`half` of the 256-column accumulator at taddr) of output tile column nt.
 template <int EPI>
-__device__ __forceinline__ void epilogue_unit(const GemmArgs& args, uint32_t taddr, long long row, int grp, int nt,
-                                              int half) {
+__device__ __forceinline__ void epilogue_unit(int32_t* ctc, uint8_t* coef, long long Mp, long long Np, int S,
+                                              uint32_t taddr, long long row, int grp, int nt, int half) {
     if (EPI == kEpiI32) {
-        int32_t* dst = args.ctc + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+        int32_t* dst = ctc + (size_t)grp * Mp * Np + (size_t)row * Np +
                        (size_t)nt * kTileN + half * (kTileN / 2);
 #pragma unroll 1
         for (int c = 0; c < kTileN / 64; ++c) {
@@ -721,8 +756,8 @@ __device__ __forceinline__ void epilogue_unit(const GemmArgs& args, uint32_t tad
         // Scheme II: reduce each INT32 residue product to its CRT
         // coefficient ((C mod m_g) * inv_g) mod m_g, one byte.
         const ModConst mc = c_mod[grp];
-        const uint32_t inv = c_crt[args.S - 1].inv[grp], c16 = c_crt[args.S - 1].c16inv[grp];
-        uint8_t* dst = args.coef + (size_t)grp * args.Mp * args.Np + (size_t)row * args.Np +
+        const uint32_t inv = c_crt[S - 1].inv[grp], c16 = c_crt[S - 1].c16inv[grp];
+        uint8_t* dst = coef + (size_t)grp * Mp * Np + (size_t)row * Np +
                        (size_t)nt * kTileN + half * (kTileN / 2);
 #pragma unroll 1
         for (int c = 0; c < kTileN / 64; ++c) {
@@ -745,10 +780,87 @@ __device__ __forceinline__ void epilogue_unit(const GemmArgs& args, uint32_t tad
     }
 }
 
-template <int EPI>
-__global__ void __launch_bounds__(kGemmThreads, 1)
-    k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-              const __grid_constant__ PairList pairs, const GemmArgs args) {
+// One work unit of the one-CTA GEMM: output tile (mt, nt) of INT32 group grp,
+// the sum over pairs [p0, p1) of A-plane x B-plane products over k_blocks.
+struct GemmUnit {
+    const CUtensorMap* tmA;
+    const CUtensorMap* tmB;
+    int p0, p1, grp, mt, nt, k_blocks, S;
+    long long Mp, Np;
+    int32_t* ctc;
+    uint8_t* coef;
+};
+
+// Work units of one GEMM: group-major, tiles rasterised in bands.
+struct SingleUnits {
+    const CUtensorMap* tmA;
+    const CUtensorMap* tmB;
+    const PairList* pairs;
+    const GemmArgs* a;
+    __device__ __forceinline__ int count() const { return a->groups * a->total_tiles; }
+    __device__ __forceinline__ void get(int u, GemmUnit& x) const {
+        x.grp = u / a->total_tiles;
+        tile_coords(u - x.grp * a->total_tiles, *a, x.mt, x.nt);
+        x.tmA = tmA;
+        x.tmB = tmB;
+        x.p0 = pairs->start[x.grp];
+        x.p1 = pairs->start[x.grp + 1];
+        x.k_blocks = a->k_blocks;
+        x.S = a->S;
+        x.Mp = a->Mp;
+        x.Np = a->Np;
+        x.ctc = a->ctc;
+        x.coef = a->coef;
+    }
+    __device__ __forceinline__ int a_plane(int p) const { return pairs->a[p]; }
+    __device__ __forceinline__ int b_plane(int p) const { return pairs->b[p]; }
+};
+
+// Work units of a group of independent Scheme II GEMMs: an explicit list of
+// (problem, mt, nt, modulus), one tensor-map pair and one coefficient buffer
+// per problem.
+struct GroupGemmProblem {
+    long long Mp, Np;
+    int k_blocks, S;
+    uint8_t* coef;
+};
+struct GroupGemmArgs {
+    const int4* units;
+    int total_units;
+    const CUtensorMap* maps;   // [2 * problems]: A planes, then B^T planes
+    const GroupGemmProblem* probs;
+    int* err;
+};
+struct GroupUnits {
+    const GroupGemmArgs* g;
+    __device__ __forceinline__ int count() const { return g->total_units; }
+    __device__ __forceinline__ void get(int u, GemmUnit& x) const {
+        const int4 w = g->units[u];
+        const GroupGemmProblem& pr = g->probs[w.x];
+        x.tmA = g->maps + 2 * w.x;
+        x.tmB = g->maps + 2 * w.x + 1;
+        x.mt = w.y;
+        x.nt = w.z;
+        x.grp = w.w;
+        x.p0 = w.w;
+        x.p1 = w.w + 1;
+        x.k_blocks = pr.k_blocks;
+        x.S = pr.S;
+        x.Mp = pr.Mp;
+        x.Np = pr.Np;
+        x.ctc = nullptr;
+        x.coef = pr.coef;
+    }
+    __device__ __forceinline__ int a_plane(int p) const { return p; }
+    __device__ __forceinline__ int b_plane(int p) const { return p; }
+};
+
+// Persistent, warp-specialised INT8 GEMM on one SM per CTA: warp 0 issues
+// TMA loads into a kStages ring, warp 1 issues tcgen05 MMAs into one of two
+// TMEM accumulators, warps 2-9 drain the other accumulator through the
+// epilogue.  CTA c takes units c, c + grid, ...  Every wait is bounded.
+template <int EPI, class Units>
+__device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -762,7 +874,6 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int G = args.groups;
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
             mbar_init(&full[i], 1);
@@ -775,8 +886,6 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         mbar_init(drain, 1);
         *abort_flag = 0;
         fence_barrier_init();
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
     }
     if (warp == 1) {
         tmem_alloc(tmem_slot, kTmemCols);
@@ -786,7 +895,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int total_units = G * args.total_tiles;
+    const int total_units = src.count();
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -794,30 +903,33 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint32_t phase = 0;
         long long issued = 0;
         bool ok = true;
+        const CUtensorMap* last_map = nullptr;
         for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
-            const int grp = u / args.total_tiles;
-            int mt, nt;
-            tile_coords(u - grp * args.total_tiles, args, mt, nt);
-            {
-                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                    const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kTileM);
-                    const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN);
-                    for (int kb = 0; kb < args.k_blocks; ++kb) {
-                        int w = 1;
-                        if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
-                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                        if (!ok) break;
-                        if (lane == 0) {
-                            mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
-                            tma_load_2d(sA + stage * kABytes, &tmA, &full[stage], kb * kTileK, arow);
-                            tma_load_2d(sB + stage * kBBytes, &tmB, &full[stage], kb * kTileK, brow);
-                        }
-                        __syncwarp();
-                        ++issued;
-                        if (++stage == kStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
+            GemmUnit x;
+            src.get(u, x);
+            if (lane == 0 && x.tmA != last_map) {
+                tma_prefetch_desc(x.tmA);
+                tma_prefetch_desc(x.tmB);
+                last_map = x.tmA;
+            }
+            for (int p = x.p0; p < x.p1 && ok; ++p) {
+                const int arow = (int)(src.a_plane(p) * x.Mp + (long long)x.mt * kTileM);
+                const int brow = (int)(src.b_plane(p) * x.Np + (long long)x.nt * kTileN);
+                for (int kb = 0; kb < x.k_blocks; ++kb) {
+                    int w = 1;
+                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, err);
+                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                    if (!ok) break;
+                    if (lane == 0) {
+                        mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
+                        tma_load_2d(sA + stage * kABytes, x.tmA, &full[stage], kb * kTileK, arow);
+                        tma_load_2d(sB + stage * kBBytes, x.tmB, &full[stage], kb * kTileK, brow);
+                    }
+                    __syncwarp();
+                    ++issued;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
                     }
                 }
             }
@@ -839,47 +951,46 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         int local = 0;
         bool ok = true;
         for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
-            const int grp = u / args.total_tiles;
-            {
-                const int acc = local & 1;
-                const uint32_t acc_phase = (local >> 1) & 1;
-                int w = 1;
-                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
-                ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                if (!ok) break;
-                tc_fence_after();
-                const uint32_t d = tmem_base + acc * kAccCols;
-                uint32_t accumulate = 0;
-                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                    for (int kb = 0; kb < args.k_blocks; ++kb) {
-                        w = 1;
-                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
-                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                        if (!ok) break;
-                        tc_fence_after();
-                        if (lane == 0) {
-                            const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
-                            const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
+            GemmUnit x;
+            src.get(u, x);
+            const int acc = local & 1;
+            const uint32_t acc_phase = (local >> 1) & 1;
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, err);
+            ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t d = tmem_base + acc * kAccCols;
+            uint32_t accumulate = 0;
+            for (int p = x.p0; p < x.p1 && ok; ++p) {
+                for (int kb = 0; kb < x.k_blocks; ++kb) {
+                    w = 1;
+                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, err);
+                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
+                    if (!ok) break;
+                    tc_fence_after();
+                    if (lane == 0) {
+                        const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
+                        const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
 #pragma unroll
-                            for (int k = 0; k < kTileK / 32; ++k) {
-                                // +32 bytes of K inside the swizzle row = +2 in 16-byte units
-                                umma_i8(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
-                                accumulate = 1;
-                            }
-                            umma_commit(&empty[stage]);
+                        for (int k = 0; k < kTileK / 32; ++k) {
+                            // +32 bytes of K inside the swizzle row = +2 in 16-byte units
+                            umma_i8(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
+                            accumulate = 1;
                         }
-                        __syncwarp();
-                        accumulate = 1;
-                        if (++stage == kStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
+                        umma_commit(&empty[stage]);
+                    }
+                    __syncwarp();
+                    accumulate = 1;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
                     }
                 }
-                if (!ok) break;
-                if (lane == 0) umma_commit(&acc_full[acc]);
-                __syncwarp();
             }
+            if (!ok) break;
+            if (lane == 0) umma_commit(&acc_full[acc]);
+            __syncwarp();
         }
         if (!ok && lane == 0) {
             // Wait for the MMAs already issued before TMEM is released.
@@ -895,28 +1006,24 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         int local = 0;
         bool ok = true;
         for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
-            const int grp = u / args.total_tiles;
-            int mt, nt;
-            tile_coords(u - grp * args.total_tiles, args, mt, nt);
-            const long long row = (long long)mt * kTileM + row_local;
-            {
-                const int acc = local & 1;
-                const uint32_t acc_phase = (local >> 1) & 1;
-                int w = 1;
-                if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
-                if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
-                    ok = false;
-                    continue;
-                }
-                tc_fence_after();
-                const uint32_t taddr =
-                    tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-                epilogue_unit<EPI>(args, taddr, row, grp, nt, half);
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&acc_empty[acc]);
-
+            GemmUnit x;
+            src.get(u, x);
+            const long long row = (long long)x.mt * kTileM + row_local;
+            const int acc = local & 1;
+            const uint32_t acc_phase = (local >> 1) & 1;
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, err);
+            if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
+                ok = false;
+                continue;
             }
+            tc_fence_after();
+            const uint32_t taddr =
+                tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
+            epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, half);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
         }
     }
 
@@ -926,6 +1033,20 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         tc_fence_after();
         tmem_dealloc(tmem_base, kTmemCols);
     }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              const __grid_constant__ PairList pairs, const __grid_constant__ GemmArgs args) {
+    const SingleUnits src{&tmA, &tmB, &pairs, &args};
+    gemm_i8_body<EPI>(src, args.err);
+}
+
+// Grouped Scheme II GEMM over an explicit unit list (coefficient epilogue).
+__global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_constant__ GroupGemmArgs g) {
+    const GroupUnits src{&g};
+    gemm_i8_body<kEpiCoef>(src, g.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -1114,7 +1235,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
             tc_fence_after();
             const uint32_t taddr =
                 tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-            epilogue_unit<EPI>(args, taddr, row, grp, nt, half);
+            epilogue_unit<EPI>(args.ctc, args.coef, args.Mp, args.Np, args.S, taddr, row, grp, nt, half);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive_cluster(empty_remote[acc]);
@@ -1136,42 +1257,49 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
 // with S fixed at compile time the table constants are instruction operands
 // and the S loads are issued together.
 template <int S>
+__device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef, long long Np, long long N,
+                                               size_t plane, const int32_t* __restrict__ sA,
+                                               const int32_t* __restrict__ sB, double* __restrict__ C,
+                                               long long chunks, long long id) {
+    constexpr int NL = (S + 3) / 4;   // 32-bit limbs of M
+    const CrtTable& T = c_crt[S - 1];
+    const long long i = id / chunks, j0 = (id - i * chunks) << 2;
+    const uint8_t* src = coef + (size_t)i * Np + j0;
+    uint32_t w[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) w[s] = __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)s * plane));
+    CrtAcc<NL> st[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) st[e].zero();
+#pragma unroll
+    for (int p = 0; p < S / 2; ++p) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            st[e].add_pair(T, p, (w[2 * p] >> (e * 8)) & 0xFFu, (w[2 * p + 1] >> (e * 8)) & 0xFFu);
+    }
+    if (S & 1) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) st[e].add(T, S - 1, (w[S - 1] >> (e * 8)) & 0xFFu);
+    }
+    const int sa = sA[i];
+    double* crow = C + i * N;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const long long j = j0 + e;
+        if (j < N) crow[j] = crt_finish<NL>(T, st[e], sa + sB[j]);
+    }
+}
+
+template <int S>
 __global__ void __launch_bounds__(256) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
                                                   long long M, long long N, const int32_t* __restrict__ sA,
                                                   const int32_t* __restrict__ sB, double* __restrict__ C) {
-    constexpr int NL = (S + 3) / 4;   // 32-bit limbs of M
     const long long chunks = (N + 3) >> 2;
     const long long total = M * chunks;
     const size_t plane = (size_t)Mp * (size_t)Np;
-    const CrtTable& T = c_crt[S - 1];
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x) {
-        const long long i = id / chunks, j0 = (id - i * chunks) << 2;
-        const uint8_t* src = coef + (size_t)i * Np + j0;
-        uint32_t w[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) w[s] = __ldg(reinterpret_cast<const uint32_t*>(src + (size_t)s * plane));
-        CrtAcc<NL> st[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) st[e].zero();
-#pragma unroll
-        for (int p = 0; p < S / 2; ++p) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                st[e].add_pair(T, p, (w[2 * p] >> (e * 8)) & 0xFFu, (w[2 * p + 1] >> (e * 8)) & 0xFFu);
-        }
-        if (S & 1) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) st[e].add(T, S - 1, (w[S - 1] >> (e * 8)) & 0xFFu);
-        }
-        const int sa = sA[i];
-        double* crow = C + i * N;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const long long j = j0 + e;
-            if (j < N) crow[j] = crt_finish<NL>(T, st[e], sa + sB[j]);
-        }
-    }
+         id += (long long)gridDim.x * blockDim.x)
+        crt_coef_chunk<S>(coef, Np, N, plane, sA, sB, C, chunks, id);
 }
 
 template <int NL>
@@ -1221,6 +1349,101 @@ __global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict_
         }
         C[id] = acc;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Grouped Scheme II: steps 1, 2 and 4 of many independent GEMMs, one launch
+// per stage (per slice-count class for the templated stages).  Block b of a
+// launch works on problem ids[q] for start[q] <= b < start[q + 1], at local
+// tile b - start[q]; the bodies are the single-GEMM kernels' own.
+// ---------------------------------------------------------------------------
+struct GroupProblemDev {
+    const double* A;
+    const double* B;
+    double* C;
+    long long M, N, K, Mp, Np, Kp;
+    int S, k_param;
+    int32_t* shiftA;
+    int32_t* shiftB;
+    unsigned long long* colmax;
+    int8_t* a_planes;
+    int8_t* b_planes;
+    uint8_t* coef;
+};
+
+struct GroupLaunchDev {
+    const int* ids;
+    const long long* start;   // n + 1 entries
+    int n;
+};
+
+// Largest q with start[q] <= b (block-uniform).
+__device__ __forceinline__ int group_find(const GroupLaunchDev& L, long long b) {
+    int lo = 0, hi = L.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(L.start + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// 8 rows per block, one warp per row.
+__global__ void __launch_bounds__(256) k_group_stats_rows(const GroupProblemDev* __restrict__ probs,
+                                                          const __grid_constant__ GroupLaunchDev L) {
+    const int q = group_find(L, blockIdx.x);
+    const GroupProblemDev& P = probs[L.ids[q]];
+    const long long r = (blockIdx.x - L.start[q]) * 8 + (threadIdx.x >> 5);
+    if (r >= P.M) return;
+    const bool vec2 = ((reinterpret_cast<uintptr_t>(P.A) & 15) == 0) && (P.K % 2 == 0);
+    const unsigned long long mx = row_max_bits(P.A + r * P.K, P.K, threadIdx.x & 31, vec2);
+    if ((threadIdx.x & 31) == 0) P.shiftA[r] = P.k_param - max_exp_from_bits(mx);
+}
+
+// Tile (strip, y0) of ceil(N/64) x ceil(K/256) per problem.
+__global__ void __launch_bounds__(256) k_group_stats_cols(const GroupProblemDev* __restrict__ probs,
+                                                          const __grid_constant__ GroupLaunchDev L) {
+    const int q = group_find(L, blockIdx.x);
+    const GroupProblemDev& P = probs[L.ids[q]];
+    const long long t = blockIdx.x - L.start[q];
+    const long long strips = (P.N + 63) / 64, ny = (P.K + 255) / 256;
+    stats_cols_block(P.B, P.K, P.N, P.colmax, t % strips, t / strips, ny);
+}
+
+// 256 chunks of 8 columns per block over the padded Mp x Kp.
+template <int SC, bool WIDE>
+__global__ void __launch_bounds__(256, 3) k_group_slice_rows(const GroupProblemDev* __restrict__ probs,
+                                                             const __grid_constant__ GroupLaunchDev L) {
+    const int q = group_find(L, blockIdx.x);
+    const GroupProblemDev& P = probs[L.ids[q]];
+    const long long id = (blockIdx.x - L.start[q]) * 256 + threadIdx.x;
+    if (id >= P.Mp * (P.Kp / 8)) return;
+    slice_rows_chunk<2, SC, WIDE>(P.A, P.M, P.K, P.shiftA, SC, 0, P.a_planes, P.Kp, (size_t)P.Mp * (size_t)P.Kp,
+                                  id);
+}
+
+// Tile (bx, by) of (Np/32) x (Kp/128) per problem.
+template <int SC, bool WIDE>
+__global__ void __launch_bounds__(256, 3) k_group_slice_cols(const GroupProblemDev* __restrict__ probs,
+                                                             const __grid_constant__ GroupLaunchDev L) {
+    const int q = group_find(L, blockIdx.x);
+    const GroupProblemDev& P = probs[L.ids[q]];
+    const long long t = blockIdx.x - L.start[q];
+    const long long nx = P.Np / 32;
+    slice_cols_tile<2, SC, WIDE>(P.B, P.K, P.N, P.colmax, P.k_param, SC, 0, P.shiftB, P.b_planes, P.Np, P.Kp, t % nx,
+                                 t / nx);
+}
+
+// 256 chunks of 4 columns per block over M x N.
+template <int S>
+__global__ void __launch_bounds__(256) k_group_crt(const GroupProblemDev* __restrict__ probs,
+                                                   const __grid_constant__ GroupLaunchDev L) {
+    const int q = group_find(L, blockIdx.x);
+    const GroupProblemDev& P = probs[L.ids[q]];
+    const long long chunks = (P.N + 3) >> 2;
+    const long long id = (blockIdx.x - L.start[q]) * 256 + threadIdx.x;
+    if (id >= P.M * chunks) return;
+    crt_coef_chunk<S>(P.coef, P.Np, P.N, (size_t)P.Mp * (size_t)P.Np, P.shiftA, P.shiftB, P.C, chunks, id);
 }
 
 // ---------------------------------------------------------------------------
@@ -1454,6 +1677,270 @@ cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t
     int grid = grid_for(total, 256, sms, 16);
     k_reconstruct1<<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, beta, negA, negB, C);
     return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Grouped plan: device tables built once, replayed by every call
+// ---------------------------------------------------------------------------
+struct GroupPlan {
+    struct Launch {
+        GroupLaunchDev dev{};
+        long long tiles = 0;
+        int S = 0;
+        bool wide = false;
+    };
+    std::vector<GroupProblemDev> probs;
+    void* dev = nullptr;
+    GroupProblemDev* d_probs = nullptr;
+    GroupGemmArgs gemm{};
+    size_t table_bytes = 0;
+    Launch rows, cols;
+    std::vector<Launch> slr, slc, crt;
+};
+
+namespace {
+
+// Byte layout of the plan's device tables, built on the host in one buffer.
+struct TableBuilder {
+    std::vector<uint8_t> buf;
+    size_t put(const void* src, size_t n, size_t align = 128) {
+        size_t off = (buf.size() + align - 1) / align * align;
+        buf.resize(off + n);
+        if (n) std::memcpy(buf.data() + off, src, n);
+        return off;
+    }
+};
+
+}  // namespace
+
+cudaError_t group_plan_prepare();
+
+cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, GroupPlan** out) {
+    *out = nullptr;
+    if (count <= 0) return cudaErrorInvalidValue;
+    {
+        const cudaError_t pe = group_plan_prepare();
+        if (pe != cudaSuccess) return pe;
+    }
+    auto* gp = new (std::nothrow) GroupPlan();
+    if (!gp) return cudaErrorMemoryAllocation;
+    std::unique_ptr<GroupPlan> hold(gp);
+    gp->probs.resize(count);
+    std::vector<GroupGemmProblem> gprobs(count);
+    std::vector<CUtensorMap> maps(2 * (size_t)count);
+    std::vector<int4> units;
+    for (int i = 0; i < count; ++i) {
+        const GroupProblem& p = in[i];
+        if (p.S < 1 || p.S > kMaxSlices || p.M == 0 || p.N == 0 || p.K == 0 || p.Mp % kTileM || p.Np % kTileN ||
+            p.Kp % kTileK)
+            return cudaErrorInvalidValue;
+        if (p.k_param > 62 && p.S < 17) return cudaErrorInvalidValue;
+        GroupProblemDev& d = gp->probs[i];
+        d.A = p.A;
+        d.B = p.B;
+        d.C = p.C;
+        d.M = (long long)p.M;
+        d.N = (long long)p.N;
+        d.K = (long long)p.K;
+        d.Mp = (long long)p.Mp;
+        d.Np = (long long)p.Np;
+        d.Kp = (long long)p.Kp;
+        d.S = p.S;
+        d.k_param = p.k_param;
+        d.shiftA = p.shiftA;
+        d.shiftB = p.shiftB;
+        d.colmax = p.colmax;
+        d.a_planes = p.a_planes;
+        d.b_planes = p.b_planes;
+        d.coef = p.coef;
+        gprobs[i] = GroupGemmProblem{d.Mp, d.Np, (int)(p.Kp / kTileK), p.S, p.coef};
+        if (!make_plane_map(&maps[2 * i], p.a_planes, (size_t)p.S * p.Mp, p.Kp, kTileM) ||
+            !make_plane_map(&maps[2 * i + 1], p.b_planes, (size_t)p.S * p.Np, p.Kp, kTileN))
+            return cudaErrorInvalidValue;
+        const int mt = (int)(p.Mp / kTileM), nt = (int)(p.Np / kTileN);
+        for (int g = 0; g < p.S; ++g)
+            for (int a = 0; a < mt; ++a)
+                for (int b = 0; b < nt; ++b) units.push_back(make_int4(i, a, b, g));
+    }
+    // Longest units first (cost ~ k_blocks): CTA c takes units c, c + grid, ...,
+    // so each round of `grid` units has near-equal cost.  Stable, so units of
+    // one problem and modulus stay together for L2 reuse.
+    std::stable_sort(units.begin(), units.end(), [&](const int4& x, const int4& y) {
+        return gprobs[x.x].k_blocks > gprobs[y.x].k_blocks;
+    });
+
+    // Per-stage block maps; the templated stages split by (S, wide) class.
+    auto tiles_of = [&](const GroupProblemDev& d, int stage) -> long long {
+        switch (stage) {
+            case 0: return (d.M + 7) / 8;
+            case 1: return ((d.N + 63) / 64) * ((d.K + 255) / 256);
+            case 2: return (d.Mp * (d.Kp / 8) + 255) / 256;
+            case 3: return (d.Np / 32) * (d.Kp / 128);
+            default: return (d.M * ((d.N + 3) / 4) + 255) / 256;
+        }
+    };
+    std::vector<std::pair<int, bool>> classes;
+    for (const auto& d : gp->probs) {
+        std::pair<int, bool> c{d.S, d.k_param > 62};
+        if (std::find(classes.begin(), classes.end(), c) == classes.end()) classes.push_back(c);
+    }
+    TableBuilder tb;
+    struct Pending {
+        GroupPlan::Launch* L;
+        size_t ids_off, start_off;
+    };
+    std::vector<Pending> pend;
+    gp->slr.resize(classes.size());
+    gp->slc.resize(classes.size());
+    gp->crt.resize(classes.size());
+    auto add_launch = [&](GroupPlan::Launch& L, int stage, int S, bool wide, bool all) {
+        std::vector<int> ids;
+        std::vector<long long> start(1, 0);
+        for (int i = 0; i < count; ++i) {
+            const GroupProblemDev& d = gp->probs[i];
+            if (!all && (d.S != S || (d.k_param > 62) != wide)) continue;
+            ids.push_back(i);
+            start.push_back(start.back() + tiles_of(d, stage));
+        }
+        L.dev.n = (int)ids.size();
+        L.tiles = start.back();
+        L.S = S;
+        L.wide = wide;
+        pend.push_back({&L, tb.put(ids.data(), ids.size() * sizeof(int)),
+                        tb.put(start.data(), start.size() * sizeof(long long))});
+    };
+    add_launch(gp->rows, 0, 0, false, true);
+    add_launch(gp->cols, 1, 0, false, true);
+    for (size_t c = 0; c < classes.size(); ++c) {
+        add_launch(gp->slr[c], 2, classes[c].first, classes[c].second, false);
+        add_launch(gp->slc[c], 3, classes[c].first, classes[c].second, false);
+        add_launch(gp->crt[c], 4, classes[c].first, classes[c].second, false);
+    }
+    for (const auto& L : {gp->rows.tiles, gp->cols.tiles})
+        if (L > 0x7FFFFFFFll) return cudaErrorInvalidValue;
+    for (size_t c = 0; c < classes.size(); ++c)
+        if (gp->slr[c].tiles > 0x7FFFFFFFll || gp->slc[c].tiles > 0x7FFFFFFFll || gp->crt[c].tiles > 0x7FFFFFFFll)
+            return cudaErrorInvalidValue;
+    if (units.size() > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const size_t probs_off = tb.put(gp->probs.data(), gp->probs.size() * sizeof(GroupProblemDev));
+    const size_t gprobs_off = tb.put(gprobs.data(), gprobs.size() * sizeof(GroupGemmProblem));
+    const size_t maps_off = tb.put(maps.data(), maps.size() * sizeof(CUtensorMap), 128);
+    const size_t units_off = tb.put(units.data(), units.size() * sizeof(int4));
+
+    cudaError_t e = cudaMalloc(&gp->dev, tb.buf.size());
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(gp->dev, tb.buf.data(), tb.buf.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(gp->dev);
+        gp->dev = nullptr;
+        return e;
+    }
+    uint8_t* base = static_cast<uint8_t*>(gp->dev);
+    for (const auto& pd : pend) {
+        pd.L->dev.ids = reinterpret_cast<const int*>(base + pd.ids_off);
+        pd.L->dev.start = reinterpret_cast<const long long*>(base + pd.start_off);
+    }
+    gp->d_probs = reinterpret_cast<GroupProblemDev*>(base + probs_off);
+    gp->gemm.units = reinterpret_cast<const int4*>(base + units_off);
+    gp->gemm.total_units = (int)units.size();
+    gp->gemm.maps = reinterpret_cast<const CUtensorMap*>(base + maps_off);
+    gp->gemm.probs = reinterpret_cast<const GroupGemmProblem*>(base + gprobs_off);
+    gp->gemm.err = err;
+    gp->table_bytes = tb.buf.size();
+    *out = hold.release();
+    return cudaSuccess;
+}
+
+void group_plan_destroy(GroupPlan* p) {
+    if (!p) return;
+    if (p->dev) cudaFree(p->dev);
+    delete p;
+}
+
+cudaError_t group_plan_set_matrices(GroupPlan* p, const double* const* A, const double* const* B,
+                                    double* const* C, cudaStream_t st) {
+    bool changed = false;
+    for (size_t i = 0; i < p->probs.size(); ++i) {
+        GroupProblemDev& d = p->probs[i];
+        if (d.A != A[i] || d.B != B[i] || d.C != C[i]) {
+            d.A = A[i];
+            d.B = B[i];
+            d.C = C[i];
+            changed = true;
+        }
+    }
+    if (!changed) return cudaSuccess;
+    // Pageable source: the copy is staged before this call returns.
+    return cudaMemcpyAsync(p->d_probs, p->probs.data(), p->probs.size() * sizeof(GroupProblemDev),
+                           cudaMemcpyHostToDevice, st);
+}
+
+size_t group_plan_units(const GroupPlan* p) { return (size_t)p->gemm.total_units; }
+size_t group_plan_table_bytes(const GroupPlan* p) { return p->table_bytes; }
+int group_plan_launches(const GroupPlan* p) { return 3 + 3 * (int)p->slr.size(); }
+
+cudaError_t group_plan_prepare() {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_group_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+    });
+    return attr;
+}
+
+cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t colmax_count, int sms,
+                              cudaStream_t st, cudaEvent_t* ev) {
+    cudaError_t e = group_plan_prepare();
+    if (e != cudaSuccess) return e;
+#define OZA_TRY(x)                          \
+    do {                                    \
+        if ((e = (x)) != cudaSuccess) return e; \
+    } while (0)
+    if (ev) OZA_TRY(cudaEventRecord(ev[0], st));
+    OZA_TRY(cudaMemsetAsync(colmax, 0, colmax_count * sizeof(unsigned long long), st));
+    k_group_stats_rows<<<(unsigned)p->rows.tiles, 256, 0, st>>>(p->d_probs, p->rows.dev);
+    k_group_stats_cols<<<(unsigned)p->cols.tiles, 256, 0, st>>>(p->d_probs, p->cols.dev);
+    OZA_TRY(cudaGetLastError());
+    if (ev) OZA_TRY(cudaEventRecord(ev[1], st));
+    for (size_t c = 0; c < p->slr.size(); ++c) {
+        const GroupPlan::Launch& R = p->slr[c];
+        const GroupPlan::Launch& Cl = p->slc[c];
+        switch (R.S) {
+#define OZA_CASE(n)                                                                                         \
+    case n:                                                                                                 \
+        if (R.wide) {                                                                                       \
+            k_group_slice_rows<n, (n >= 17)><<<(unsigned)R.tiles, 256, 0, st>>>(p->d_probs, R.dev);       \
+            k_group_slice_cols<n, (n >= 17)><<<(unsigned)Cl.tiles, 256, 0, st>>>(p->d_probs, Cl.dev);     \
+        } else {                                                                                            \
+            k_group_slice_rows<n, false><<<(unsigned)R.tiles, 256, 0, st>>>(p->d_probs, R.dev);            \
+            k_group_slice_cols<n, false><<<(unsigned)Cl.tiles, 256, 0, st>>>(p->d_probs, Cl.dev);          \
+        }                                                                                                   \
+        break;
+            OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+            default: return cudaErrorInvalidValue;
+        }
+        OZA_TRY(cudaGetLastError());
+    }
+    if (ev) OZA_TRY(cudaEventRecord(ev[2], st));
+    const int grid = p->gemm.total_units < sms ? p->gemm.total_units : sms;
+    if (grid > 0) k_group_gemm_i8<<<grid, kGemmThreads, kGemmSmem, st>>>(p->gemm);
+    OZA_TRY(cudaGetLastError());
+    if (ev) OZA_TRY(cudaEventRecord(ev[3], st));
+    for (const GroupPlan::Launch& L : p->crt) {
+        switch (L.S) {
+#define OZA_CASE(n) \
+    case n: k_group_crt<n><<<(unsigned)L.tiles, 256, 0, st>>>(p->d_probs, L.dev); break;
+            OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+            default: return cudaErrorInvalidValue;
+        }
+        OZA_TRY(cudaGetLastError());
+    }
+    if (ev) OZA_TRY(cudaEventRecord(ev[4], st));
+#undef OZA_TRY
+    return cudaSuccess;
 }
 
 }  // namespace oza

@@ -76,6 +76,35 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
                                 const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st);
 
+// Grouped Scheme II: many independent GEMMs, each stage one launch (the
+// slicers and the CRT one per slice-count class).  Buffers as in a Scheme II
+// workspace, per problem; colmax of all problems is one contiguous array.
+struct GroupProblem {
+    const double* A;
+    const double* B;
+    double* C;
+    size_t M, N, K, Mp, Np, Kp;
+    int S, k_param;
+    int32_t* shiftA;
+    int32_t* shiftB;
+    unsigned long long* colmax;
+    int8_t* a_planes;   // [S][Mp][Kp]
+    int8_t* b_planes;   // [S][Np][Kp]
+    uint8_t* coef;      // [S][Mp][Np]
+};
+struct GroupPlan;   // device tables: problems, per-stage block maps, GEMM work units, tensor maps
+cudaError_t group_plan_create(const GroupProblem* probs, int count, int* err, GroupPlan** out);
+void group_plan_destroy(GroupPlan* p);
+// New A/B/C pointers for the next launches (stream-ordered upload when changed).
+cudaError_t group_plan_set_matrices(GroupPlan* p, const double* const* A, const double* const* B,
+                                    double* const* C, cudaStream_t st);
+// Steps 1-4 of every problem; ev (optional) = 5 events bracketing the steps.
+cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t colmax_count, int sms,
+                              cudaStream_t st, cudaEvent_t* ev);
+size_t group_plan_units(const GroupPlan* p);
+size_t group_plan_table_bytes(const GroupPlan* p);
+int group_plan_launches(const GroupPlan* p);   // kernel launches per call
+
 // Sets the text returned by oza_last_error_string() on this thread.
 void set_last_error(const char* msg);
 

@@ -117,3 +117,13 @@ def test_accuracy_tools_reject_null_arguments():
                                  ctypes.byref(e)) == oz.OZA_INVALID_ARG
     assert L.oza_block_error(None, None, None, None, 4, 4, 4, 8, 0, ctypes.byref(e)) == oz.OZA_INVALID_ARG
     assert "null" in L.oza_last_error_string().decode()
+
+
+def test_group_api_rejects_bad_arguments_without_a_device():
+    L = oz.lib()
+    h = ctypes.c_void_p()
+    one = (ctypes.c_size_t * 1)(4)
+    s = (ctypes.c_int * 1)(8)
+    assert L.oza_group_create(None, 2, 1, one, one, one, s, 0, ctypes.byref(h)) == oz.OZA_INVALID_ARG
+    assert L.oza_group_gemm(None, None, None, None, None) == oz.OZA_INVALID_ARG
+    assert L.oza_group_destroy(None) == oz.OZA_OK
