@@ -52,11 +52,14 @@ def parse():
     p.add_argument("--phi", type=float, default=0.5)
     p.add_argument("--cpu-sample", type=int, default=512, help="rows/cols of the CPU block sample")
     p.add_argument("--no-extras", action="store_true", help="skip DGEMM / reference-GPU / accuracy side numbers")
-    p.add_argument("--suite", default=None, choices=["precision", "grouped"],
+    p.add_argument("--suite", default=None, choices=["precision", "grouped", "serve"],
                    help="precision: precision-targeted rectangular GEMMs with the slice count autotuned to "
                         "native DGEMM's error (one JSON line per shape and scheme); grouped: 512 independent "
                         "GEMMs as one grouped launch replayed from a CUDA graph vs 512 plain calls")
     p.add_argument("--group-count", type=int, default=512)
+    p.add_argument("--serve-requests", type=int, default=600)
+    p.add_argument("--serve-loads", type=str, default="0.5,0.8,0.95",
+                   help="offered loads as fractions of the batched server's measured capacity")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
     return p.parse_args()
@@ -695,8 +698,190 @@ def run_grouped_suite(args, local):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ serving suite
+SERVE_BUDGET = 120 << 30
+SERVE_WS_CAP = 2 << 30
+
+
+def serve_requests(n, seed=99):
+    """M, N, K log-uniform in [128, 8192] (K capped so the workspace is at most
+    2 GiB), phi in {0.5, 2}, target in {1e-12, 1e-15} -> slice count from the
+    calibrated table (20 where it is not reached)."""
+    import numpy as np
+    import ozablas_b200 as oz
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        M, N, K = (int(v) for v in np.rint(np.exp(rng.uniform(math.log(128), math.log(8192), 3))))
+        phi = float(rng.choice([0.5, 2.0]))
+        target = float(rng.choice([1e-12, 1e-15]))
+        S = oz.slices_for_target(target, K, phi)
+        while oz.Server.request_bytes(M, N, K, min(S, 20)) > SERVE_WS_CAP and K > 128:
+            K = max(128, K * 3 // 4)
+            S = oz.slices_for_target(target, K, phi)
+        out.append(dict(M=M, N=N, K=K, phi=phi, target=target, S=min(S, 20), table_reaches_target=S <= 20))
+    return out
+
+
+def run_serve_suite(args, local):
+    """Served DGEMM stream: Poisson arrivals at offered loads swept as
+    fractions of the batched server's capacity; the request loop (continuous
+    batching into the grouped kernels, 120 GiB workspace budget) against a
+    FIFO of per-request plain calls (workspace + oza_gemm + synchronise)."""
+    import numpy as np
+    import torch
+    import ozablas_b200 as oz
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ex = oz.CudaExecutor(local)
+    reqs = serve_requests(args.serve_requests)
+    # Input pools, one per phi: requests read M x K / K x N windows of them.
+    g = torch.Generator(device=dev).manual_seed(5)
+    pool = {}
+    for phi in (0.5, 2.0):
+        n = 8192 * 8192
+        pool[phi] = [((torch.rand(n, generator=g, device=dev, dtype=torch.float64) - 0.5)
+                      * torch.exp(phi * torch.randn(n, generator=g, device=dev, dtype=torch.float64)))
+                     for _ in range(2)]
+    rng = np.random.default_rng(17)
+    A, B, C = [], [], []
+    for r in reqs:
+        pa, pb = pool[r["phi"]]
+        oa = int(rng.integers(0, (pa.numel() - r["M"] * r["K"]) // 2 + 1)) * 2
+        ob = int(rng.integers(0, (pb.numel() - r["K"] * r["N"]) // 2 + 1)) * 2
+        A.append(pa[oa:oa + r["M"] * r["K"]].view(r["M"], r["K"]))
+        B.append(pb[ob:ob + r["K"] * r["N"]].view(r["K"], r["N"]))
+        C.append(torch.empty(r["M"], r["N"], dtype=torch.float64, device=dev))
+    torch.cuda.synchronize()
+    flops = [2.0 * r["M"] * r["N"] * r["K"] for r in reqs]
+    total_flops = sum(flops)
+
+    def served(arrivals):
+        """Submit request i at arrivals[i] (seconds from start); returns per-request
+        latencies (s) and the makespan."""
+        srv = oz.Server(ex, SERVE_BUDGET, max_inflight=2, max_batch=64)
+        try:
+            ids = [None] * len(reqs)
+            t0 = time.perf_counter()
+            for i, r in enumerate(reqs):
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids[i] = srv.submit(A[i], B[i], C[i], r["S"])
+            st = [srv.wait(i, timeout=600) for i in ids]
+            sst = srv.stats()
+        finally:
+            srv.close()
+        lat = [x["done_s"] - x["submit_s"] for x in st]
+        span = max(x["done_s"] for x in st) - min(x["submit_s"] for x in st)
+        return lat, span, sst, st
+
+    def service_times():
+        """Device time of each request alone through oza_gemm (workspace made
+        beforehand, second call timed with events)."""
+        out = []
+        for i, r in enumerate(reqs):
+            ws = oz.WorkspaceScheme2(ex, r["M"], r["N"], r["K"], r["S"])
+            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i])
+            t = oz.OzaTimings()
+            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i], t)
+            out.append(t.total_ms * 1e-3)
+            del ws
+        return out
+
+    def fifo(arrivals, service):
+        """Single-server FIFO replay: start = max(arrival, previous finish)."""
+        lat, fin = [], 0.0
+        for a, sv in zip(arrivals, service):
+            fin = max(a, fin) + sv
+            lat.append(fin - a)
+        return lat, fin - arrivals[0]
+
+    def plain(arrivals):
+        """One worker, FIFO: a workspace per request, oza_gemm, synchronise."""
+        lat = []
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if arrivals[i] > now:
+                time.sleep(arrivals[i] - now)
+            ws = oz.WorkspaceScheme2(ex, r["M"], r["N"], r["K"], r["S"])
+            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i])
+            ex.synchronize()
+            del ws
+            lat.append(time.perf_counter() - t0 - arrivals[i])
+        span = time.perf_counter() - t0
+        return lat, span
+
+    # warm-up (module loads, first launches), then capacity: everything at t = 0
+    zero = [0.0] * len(reqs)
+    served([0.0] * len(reqs))
+    lat0, span0, sst0, _ = served(zero)
+    capacity_rps = len(reqs) / span0
+    C_served = [c.clone() for c in C[:16]]
+    plat0, pspan0 = plain(zero)
+    service = service_times()
+    rlat0, rspan0 = fifo(zero, service)
+    identical = all(torch.equal(a.view(torch.int64), b.view(torch.int64)) for a, b in zip(C_served, C[:16]))
+
+    # accuracy of 16 sampled requests against their targets (double-double reference)
+    acc = []
+    for i in rng.choice(len(reqs), 16, replace=False):
+        r = reqs[i]
+        e = oz.block_error(ex, A[i], B[i], C[i], r["M"], r["N"], r["K"], 128, 3)
+        acc.append({"target": r["target"], "slices": r["S"], "err": e, "met": e <= r["target"],
+                    "table_reaches_target": r["table_reaches_target"]})
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x) * 1e3, q))
+
+    base = {
+        "suite": "serve", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
+        "config": {"workload": f"served_dgemm_stream_{len(reqs)}_requests",
+                   "dims": "M, N, K log-uniform in [128, 8192], K capped so the workspace is <= 2 GiB",
+                   "phi": [0.5, 2.0], "targets": [1e-12, 1e-15],
+                   "slices": "oza_slices_for_target (20 where the table does not reach the target)",
+                   "budget_bytes": SERVE_BUDGET, "max_inflight": 2, "max_batch": 64,
+                   "total_gflop": total_flops / 1e9, "request_seed": 99},
+    }
+    print(json.dumps(dict(base, load="capacity (all requests at t=0)",
+                          value=total_flops / span0 / 1e12,
+                          served={"tflops": total_flops / span0 / 1e12, "p50_ms": pct(lat0, 50),
+                                  "p99_ms": pct(lat0, 99), "requests_per_s": capacity_rps,
+                                  "batches": sst0["batches"], "max_batch": sst0["max_batch_seen"],
+                                  "arena_peak_bytes": sst0["arena_peak"]},
+                          plain={"tflops": total_flops / pspan0 / 1e12, "p50_ms": pct(plat0, 50),
+                                 "p99_ms": pct(plat0, 99), "requests_per_s": len(reqs) / pspan0,
+                                 "what": "FIFO worker: workspace created per request, oza_gemm, synchronise"},
+                          plain_resident={"tflops": total_flops / rspan0 / 1e12, "p50_ms": pct(rlat0, 50),
+                                          "p99_ms": pct(rlat0, 99), "requests_per_s": len(reqs) / rspan0,
+                                          "what": "FIFO replay of each request's measured oza_gemm device "
+                                                  "time, workspaces resident (no allocation cost)"},
+                          served_equals_plain_bits=identical, accuracy_sampled=acc)), flush=True)
+    for frac in (float(x) for x in args.serve_loads.split(",")):
+        lam = frac * capacity_rps
+        gaps = np.random.default_rng(1000 + int(frac * 100)).exponential(1.0 / lam, len(reqs))
+        arrivals = list(np.cumsum(gaps) - gaps[0])
+        lat, span, sst, _ = served(arrivals)
+        plat, pspan = plain(arrivals)
+        rlat, rspan = fifo(arrivals, service)
+        print(json.dumps(dict(base, load=f"{frac:.2f} x capacity ({lam:.1f} req/s Poisson)",
+                              value=total_flops / span / 1e12,
+                              served={"tflops": total_flops / span / 1e12, "p50_ms": pct(lat, 50),
+                                      "p99_ms": pct(lat, 99), "batches": sst["batches"],
+                                      "max_batch": sst["max_batch_seen"]},
+                              plain={"tflops": total_flops / pspan / 1e12, "p50_ms": pct(plat, 50),
+                                     "p99_ms": pct(plat, 99)},
+                              plain_resident={"tflops": total_flops / rspan / 1e12, "p50_ms": pct(rlat, 50),
+                                              "p99_ms": pct(rlat, 99)})), flush=True)
+
+
 def main():
     args = parse()
+    if args.suite == "serve":
+        run_serve_suite(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     if args.suite == "grouped":
         run_grouped_suite(args, int(os.environ.get("LOCAL_RANK", 0)))
         return

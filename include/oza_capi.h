@@ -177,6 +177,50 @@ oza_status_t oza_group_gemm(oza_group_t g, const double* const* A, const double*
 oza_status_t oza_group_get_info(oza_group_t g, oza_group_info_t* info);
 oza_status_t oza_group_device_error(oza_group_t g, int* code);
 
+/* ---- request loop ---------------------------------------------------------- */
+/* A server for streams of independent Scheme II FP64 GEMMs with continuous
+ * batching.  Requests are admitted in arrival order while their workspaces fit
+ * in a device arena of `workspace_budget` bytes (allocated at creation) and one
+ * of `max_inflight` stream slots is free; everything admitted together runs as
+ * one grouped batch (the oza_group kernels).  Batches on different slots
+ * overlap on the device.  Each result is bit-identical to oza_gemm on the same
+ * request alone.  Extension: the reference has no request loop. */
+typedef struct oza_server* oza_server_t;
+
+typedef struct {
+    size_t workspace_budget; /* bytes of device memory for request workspaces */
+    int max_inflight;        /* batches on the GPU at once (1..16) */
+    int max_batch;           /* requests per batch */
+} oza_server_config_t;
+
+typedef struct {
+    double submit_s, admit_s, done_s; /* host clock, seconds since server creation */
+    int slices;
+    int batch_size;                   /* requests in the batch that ran it */
+    int status;                       /* oza_status_t of the request */
+    size_t workspace_bytes;
+} oza_request_stats_t;
+
+typedef struct {
+    size_t submitted, admitted, completed, queued, batches;
+    int max_batch_seen;
+    size_t arena_used, arena_peak, workspace_budget;
+} oza_server_stats_t;
+
+oza_status_t oza_server_create(oza_exec_t ex, const oza_server_config_t* cfg, oza_server_t* out);
+/* Runs every queued request to completion, then frees the server. */
+oza_status_t oza_server_destroy(oza_server_t s);
+/* Queue C = A * B (row-major device buffers, valid until the request
+ * completes).  OZA_OOM if the request alone exceeds the budget. */
+oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, const double* A, const double* B,
+                               double* C, int slices, uint64_t* id);
+/* Wait for a request (timeout_s < 0: no limit; OZA_TIMEOUT if it expires) and
+ * release its record; stats (optional) receives its timestamps. */
+oza_status_t oza_server_wait(oza_server_t s, uint64_t id, double timeout_s, oza_request_stats_t* stats);
+oza_status_t oza_server_get_stats(oza_server_t s, oza_server_stats_t* out);
+/* Workspace bytes one request takes from the arena (0 for invalid sizes). */
+size_t oza_server_request_bytes(size_t M, size_t N, size_t K, int slices);
+
 /* ---- accuracy tools ------------------------------------------------------- */
 /* Maximum relative error of C (M x N, device) against a double-double
  * reference of the same entries, over a seeded sample of `block` rows x `block`
@@ -195,6 +239,15 @@ oza_status_t oza_block_error(oza_exec_t ex, const double* A, const double* B, co
 oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, const double* A,
                                  const double* B, double target_rel_err, int block, unsigned seed, int* slices,
                                  double* achieved_err);
+
+/* Slice count for a maximum-relative-error target without running anything:
+ * a table measured on B200 (ozablas_b200/calibrate_slices.py) for K = 128 ..
+ * 65536 and inputs (U - 0.5) * exp(phi * N(0,1)), phi = 0.5 .. 4, errors over
+ * 256 x 256 outputs against a double-double reference; the monotone envelope
+ * over K' <= K and phi' <= phi is taken.  Returns 1..20, 21 if 20 slices did
+ * not reach the target at the calibrated points, 0 for invalid arguments.
+ * Extension: the reference leaves `slices` to the caller. */
+int oza_slices_for_target(double target_rel_err, size_t K, double phi);
 
 /* ---- host utilities ------------------------------------------------------- */
 /* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from

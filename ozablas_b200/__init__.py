@@ -26,7 +26,7 @@ __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
-    "autotune_slices", "GroupGemm",
+    "autotune_slices", "GroupGemm", "Server", "slices_for_target",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -64,6 +64,23 @@ class _WsInfo(ctypes.Structure):
 class _GroupInfo(ctypes.Structure):
     _fields_ = [("count", ctypes.c_size_t), ("units", ctypes.c_size_t), ("bytes", ctypes.c_size_t),
                 ("launches", ctypes.c_int), ("graph", ctypes.c_int)]
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("workspace_budget", ctypes.c_size_t), ("max_inflight", ctypes.c_int), ("max_batch", ctypes.c_int)]
+
+
+class _RequestStats(ctypes.Structure):
+    _fields_ = [("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("slices", ctypes.c_int), ("batch_size", ctypes.c_int), ("status", ctypes.c_int),
+                ("workspace_bytes", ctypes.c_size_t)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_size_t), ("admitted", ctypes.c_size_t), ("completed", ctypes.c_size_t),
+                ("queued", ctypes.c_size_t), ("batches", ctypes.c_size_t), ("max_batch_seen", ctypes.c_int),
+                ("arena_used", ctypes.c_size_t), ("arena_peak", ctypes.c_size_t),
+                ("workspace_budget", ctypes.c_size_t)]
 
 
 @dataclass
@@ -120,6 +137,13 @@ def lib() -> ctypes.CDLL:
                                ctypes.POINTER(_Timings)]),
         "oza_group_get_info": (I, [P, ctypes.POINTER(_GroupInfo)]),
         "oza_group_device_error": (I, [P, ctypes.POINTER(I)]),
+        "oza_server_create": (I, [P, ctypes.POINTER(_ServerConfig), ctypes.POINTER(P)]),
+        "oza_server_destroy": (I, [P]),
+        "oza_server_submit": (I, [P, S, S, S, P, P, P, I, ctypes.POINTER(ctypes.c_uint64)]),
+        "oza_server_wait": (I, [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_RequestStats)]),
+        "oza_server_get_stats": (I, [P, ctypes.POINTER(_ServerStats)]),
+        "oza_server_request_bytes": (S, [S, S, S, I]),
+        "oza_slices_for_target": (I, [ctypes.c_double, S, ctypes.c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -380,6 +404,71 @@ class GroupGemm:
             self._h = None
 
 
+class Server:
+    """Request loop with continuous batching for Scheme II FP64 GEMMs
+    (extension; the reference has no request loop).  Requests are admitted in
+    arrival order while their workspaces fit in `workspace_budget` bytes of
+    device memory and one of `max_inflight` stream slots is free; each batch
+    runs the grouped kernels.
+
+        srv = Server(ex, 8 << 30)
+        rid = srv.submit(A, B, C, slices=16)   # device matrices, kept alive by the caller
+        stats = srv.wait(rid)                  # timestamps in seconds since creation
+    """
+
+    def __init__(self, executor, workspace_budget: int, max_inflight: int = 2, max_batch: int = 64):
+        if not isinstance(executor, CudaExecutor):
+            raise OzaError("OzaBLAS: No suitable hardware backend found for the provided Executor.")
+        self._exec = executor
+        cfg = _ServerConfig(int(workspace_budget), int(max_inflight), int(max_batch))
+        h = ctypes.c_void_p()
+        _check(lib().oza_server_create(executor.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def request_bytes(M: int, N: int, K: int, slices: int) -> int:
+        return int(lib().oza_server_request_bytes(int(M), int(N), int(K), int(slices)))
+
+    def submit(self, A, B, C, slices: int, M: int | None = None, N: int | None = None,
+               K: int | None = None) -> int:
+        if M is None:
+            M, K = A.shape
+            N = B.shape[1]
+            if tuple(B.shape) != (K, N) or tuple(C.shape) != (M, N):
+                raise ValueError("shapes do not agree")
+        rid = ctypes.c_uint64()
+        _check(lib().oza_server_submit(self._h, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
+                                       ctypes.c_void_p(_ptr(B)), ctypes.c_void_p(_ptr(C)), int(slices),
+                                       ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid: int, timeout: float | None = None) -> dict:
+        st = _RequestStats()
+        _check(lib().oza_server_wait(self._h, int(rid), -1.0 if timeout is None else float(timeout),
+                                     ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _RequestStats._fields_}
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(lib().oza_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.oza_server_destroy(h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+
 def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):
     """Seeded (U-0.5)*exp(phi*N(0,1)) matrix as a numpy array (reference
     generate_ozaki_matrix, utils/matrix_gen.hpp:15-34)."""
@@ -410,6 +499,15 @@ def autotune_slices(executor, scheme: int, A, B, M: int, N: int, K: int, target_
                                      ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)), float(target_rel_err),
                                      int(block), int(seed), ctypes.byref(s), ctypes.byref(e)))
     return s.value, e.value
+
+
+def slices_for_target(target_rel_err: float, K: int, phi: float = 2.0) -> int:
+    """Scheme II slice count for a maximum-relative-error target from the
+    calibrated table (no GPU work); 21 means 20 slices did not reach it."""
+    s = int(lib().oza_slices_for_target(float(target_rel_err), int(K), float(phi)))
+    if s == 0:
+        raise ValueError("target must be > 0, K >= 1, phi >= 0")
+    return s
 
 
 def scheme1_beta(K: int) -> int:

@@ -1689,14 +1689,23 @@ struct GroupPlan {
         long long tiles = 0;
         int S = 0;
         bool wide = false;
+        size_t ids_off = 0, start_off = 0;   // in the table image
     };
     std::vector<GroupProblemDev> probs;
-    void* dev = nullptr;
+    std::vector<uint8_t> image;           // host image of the device tables
+    size_t probs_off = 0, gprobs_off = 0, maps_off = 0, units_off = 0;
+    void* dev = nullptr;                  // owned table memory (group_plan_create only)
     GroupProblemDev* d_probs = nullptr;
     GroupGemmArgs gemm{};
     size_t table_bytes = 0;
     Launch rows, cols;
     std::vector<Launch> slr, slc, crt;
+    std::vector<Launch*> all_launches() {
+        std::vector<Launch*> v{&rows, &cols};
+        for (auto* vec : {&slr, &slc, &crt})
+            for (auto& L : *vec) v.push_back(&L);
+        return v;
+    }
 };
 
 namespace {
@@ -1704,6 +1713,7 @@ namespace {
 // Byte layout of the plan's device tables, built on the host in one buffer.
 struct TableBuilder {
     std::vector<uint8_t> buf;
+    TableBuilder() { buf.reserve(1 << 16); }
     size_t put(const void* src, size_t n, size_t align = 128) {
         size_t off = (buf.size() + align - 1) / align * align;
         buf.resize(off + n);
@@ -1716,7 +1726,7 @@ struct TableBuilder {
 
 cudaError_t group_plan_prepare();
 
-cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, GroupPlan** out) {
+cudaError_t group_plan_build(const GroupProblem* in, int count, int* err, GroupPlan** out) {
     *out = nullptr;
     if (count <= 0) return cudaErrorInvalidValue;
     {
@@ -1786,11 +1796,6 @@ cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, Group
         if (std::find(classes.begin(), classes.end(), c) == classes.end()) classes.push_back(c);
     }
     TableBuilder tb;
-    struct Pending {
-        GroupPlan::Launch* L;
-        size_t ids_off, start_off;
-    };
-    std::vector<Pending> pend;
     gp->slr.resize(classes.size());
     gp->slc.resize(classes.size());
     gp->crt.resize(classes.size());
@@ -1807,8 +1812,8 @@ cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, Group
         L.tiles = start.back();
         L.S = S;
         L.wide = wide;
-        pend.push_back({&L, tb.put(ids.data(), ids.size() * sizeof(int)),
-                        tb.put(start.data(), start.size() * sizeof(long long))});
+        L.ids_off = tb.put(ids.data(), ids.size() * sizeof(int));
+        L.start_off = tb.put(start.data(), start.size() * sizeof(long long));
     };
     add_launch(gp->rows, 0, 0, false, true);
     add_launch(gp->cols, 1, 0, false, true);
@@ -1823,32 +1828,44 @@ cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, Group
         if (gp->slr[c].tiles > 0x7FFFFFFFll || gp->slc[c].tiles > 0x7FFFFFFFll || gp->crt[c].tiles > 0x7FFFFFFFll)
             return cudaErrorInvalidValue;
     if (units.size() > 0x7FFFFFFFull) return cudaErrorInvalidValue;
-    const size_t probs_off = tb.put(gp->probs.data(), gp->probs.size() * sizeof(GroupProblemDev));
-    const size_t gprobs_off = tb.put(gprobs.data(), gprobs.size() * sizeof(GroupGemmProblem));
-    const size_t maps_off = tb.put(maps.data(), maps.size() * sizeof(CUtensorMap), 128);
-    const size_t units_off = tb.put(units.data(), units.size() * sizeof(int4));
+    gp->probs_off = tb.put(gp->probs.data(), gp->probs.size() * sizeof(GroupProblemDev));
+    gp->gprobs_off = tb.put(gprobs.data(), gprobs.size() * sizeof(GroupGemmProblem));
+    gp->maps_off = tb.put(maps.data(), maps.size() * sizeof(CUtensorMap), 128);
+    gp->units_off = tb.put(units.data(), units.size() * sizeof(int4));
+    gp->gemm.total_units = (int)units.size();
+    gp->gemm.err = err;
+    gp->image.swap(tb.buf);
+    gp->table_bytes = gp->image.size();
+    *out = hold.release();
+    return cudaSuccess;
+}
 
-    cudaError_t e = cudaMalloc(&gp->dev, tb.buf.size());
+void group_plan_bind(GroupPlan* gp, void* dev) {
+    uint8_t* base = static_cast<uint8_t*>(dev);
+    for (GroupPlan::Launch* L : gp->all_launches()) {
+        L->dev.ids = reinterpret_cast<const int*>(base + L->ids_off);
+        L->dev.start = reinterpret_cast<const long long*>(base + L->start_off);
+    }
+    gp->d_probs = reinterpret_cast<GroupProblemDev*>(base + gp->probs_off);
+    gp->gemm.units = reinterpret_cast<const int4*>(base + gp->units_off);
+    gp->gemm.maps = reinterpret_cast<const CUtensorMap*>(base + gp->maps_off);
+    gp->gemm.probs = reinterpret_cast<const GroupGemmProblem*>(base + gp->gprobs_off);
+}
+
+const void* group_plan_image(const GroupPlan* p) { return p->image.data(); }
+
+cudaError_t group_plan_create(const GroupProblem* in, int count, int* err, GroupPlan** out) {
+    GroupPlan* gp = nullptr;
+    cudaError_t e = group_plan_build(in, count, err, &gp);
     if (e != cudaSuccess) return e;
-    e = cudaMemcpy(gp->dev, tb.buf.data(), tb.buf.size(), cudaMemcpyHostToDevice);
+    e = cudaMalloc(&gp->dev, gp->table_bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(gp->dev, gp->image.data(), gp->table_bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        cudaFree(gp->dev);
-        gp->dev = nullptr;
+        group_plan_destroy(gp);
         return e;
     }
-    uint8_t* base = static_cast<uint8_t*>(gp->dev);
-    for (const auto& pd : pend) {
-        pd.L->dev.ids = reinterpret_cast<const int*>(base + pd.ids_off);
-        pd.L->dev.start = reinterpret_cast<const long long*>(base + pd.start_off);
-    }
-    gp->d_probs = reinterpret_cast<GroupProblemDev*>(base + probs_off);
-    gp->gemm.units = reinterpret_cast<const int4*>(base + units_off);
-    gp->gemm.total_units = (int)units.size();
-    gp->gemm.maps = reinterpret_cast<const CUtensorMap*>(base + maps_off);
-    gp->gemm.probs = reinterpret_cast<const GroupGemmProblem*>(base + gprobs_off);
-    gp->gemm.err = err;
-    gp->table_bytes = tb.buf.size();
-    *out = hold.release();
+    group_plan_bind(gp, gp->dev);
+    *out = gp;
     return cudaSuccess;
 }
 

@@ -94,6 +94,11 @@ struct GroupProblem {
 };
 struct GroupPlan;   // device tables: problems, per-stage block maps, GEMM work units, tensor maps
 cudaError_t group_plan_create(const GroupProblem* probs, int count, int* err, GroupPlan** out);
+// The same tables without device memory: a host image of group_plan_table_bytes()
+// (group_plan_image) that the caller copies to device memory it owns, then binds.
+cudaError_t group_plan_build(const GroupProblem* probs, int count, int* err, GroupPlan** out);
+const void* group_plan_image(const GroupPlan* p);
+void group_plan_bind(GroupPlan* p, void* dev_tables);
 void group_plan_destroy(GroupPlan* p);
 // New A/B/C pointers for the next launches (stream-ordered upload when changed).
 cudaError_t group_plan_set_matrices(GroupPlan* p, const double* const* A, const double* const* B,

@@ -12,6 +12,7 @@
 
 #include "oza_capi.h"
 #include "oza_kernels.h"
+#include "oza_slice_table.h"
 
 namespace oza {
 cudaError_t launch_dd_block_gemm(const double* A, const double* B, int r, int c, size_t K, double* C,
@@ -195,6 +196,28 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
     *slices = hi;
     if (achieved_err) *achieved_err = best_err;
     return OZA_OK;
+}
+
+int oza_slices_for_target(double target_rel_err, size_t K, double phi) {
+    if (!(target_rel_err > 0.0) || K == 0 || !(phi >= 0.0)) return 0;
+    // Decade: the smallest d with 10^-d <= target (conservative), clamped to the table.
+    int d = (int)std::ceil(-std::log10(target_rel_err) - 1e-9);
+    if (d < kSliceTableDecadeMin) d = kSliceTableDecadeMin;
+    if (d > kSliceTableDecadeMax) return 21;
+    const int nk = (int)(sizeof(kSliceTableK) / sizeof(kSliceTableK[0]));
+    const int np = (int)(sizeof(kSliceTablePhi) / sizeof(kSliceTablePhi[0]));
+    int ki = 0;
+    while (ki < nk - 1 && (size_t)kSliceTableK[ki] < K) ++ki;
+    int extra = 0;   // beyond the last K: one more slice per factor 4
+    for (size_t k = (size_t)kSliceTableK[nk - 1]; k < K; k *= 4) ++extra;
+    int pi = 0;
+    while (pi < np - 1 && kSliceTablePhi[pi] < phi) ++pi;
+    // Monotone envelope: the measured maximum error is noisy in K and phi.
+    int S = 1;
+    for (int a = 0; a <= ki; ++a)
+        for (int b = 0; b <= pi; ++b) S = std::max(S, (int)kSliceTable[a][b][d - kSliceTableDecadeMin]);
+    S += extra;
+    return S > 21 ? 21 : S;
 }
 
 }  // extern "C"

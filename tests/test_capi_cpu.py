@@ -127,3 +127,40 @@ def test_group_api_rejects_bad_arguments_without_a_device():
     assert L.oza_group_create(None, 2, 1, one, one, one, s, 0, ctypes.byref(h)) == oz.OZA_INVALID_ARG
     assert L.oza_group_gemm(None, None, None, None, None) == oz.OZA_INVALID_ARG
     assert L.oza_group_destroy(None) == oz.OZA_OK
+
+
+def test_server_api_without_a_device():
+    L = oz.lib()
+    h = ctypes.c_void_p()
+    assert L.oza_server_create(None, None, ctypes.byref(h)) == oz.OZA_INVALID_ARG
+    rid = ctypes.c_uint64()
+    assert L.oza_server_submit(None, 4, 4, 4, None, None, None, 8, ctypes.byref(rid)) == oz.OZA_INVALID_ARG
+    assert L.oza_server_destroy(None) == oz.OZA_OK
+
+
+def test_server_request_bytes_layout():
+    """Workspace of one request: shifts, S x (Mp Kp + Np Kp + Mp Np), each part
+    rounded to 1 KiB; tiles 128 (M), 256 (N), 128 (K)."""
+    ru = lambda x, m: (x + m - 1) // m * m   # noqa: E731
+    for M, N, K, S in [(1, 1, 1, 1), (100, 300, 77, 16), (8192, 8192, 1000, 20)]:
+        Mp, Np, Kp = ru(M, 128), ru(N, 256), ru(K, 128)
+        want = sum(ru(x, 1024) for x in (4 * M, 4 * N, S * Mp * Kp, S * Np * Kp, S * Mp * Np))
+        assert oz.Server.request_bytes(M, N, K, S) == want
+    assert oz.Server.request_bytes(0, 4, 4, 8) == 0
+    assert oz.Server.request_bytes(4, 4, 4, 21) == 0
+
+
+def test_slices_for_target_is_a_monotone_lookup():
+    f = oz.slices_for_target
+    for phi in (0.5, 1.0, 2.0, 4.0):
+        for t in (1e-9, 1e-12, 1e-15):
+            s = [f(t, K, phi) for K in (100, 128, 1000, 4096, 65536, 10 ** 6)]
+            assert s == sorted(s) and all(1 <= x <= 21 for x in s)
+    for K in (256, 8192):
+        assert [f(1e-12, K, p) for p in (0.1, 0.5, 1.0, 2.0, 4.0, 9.0)] == sorted(
+            f(1e-12, K, p) for p in (0.1, 0.5, 1.0, 2.0, 4.0, 9.0))
+        assert [f(t, K, 1.0) for t in (1e-6, 1e-9, 1e-12, 1e-14)] == sorted(
+            f(t, K, 1.0) for t in (1e-6, 1e-9, 1e-12, 1e-14))
+    assert f(1e-17, 1024, 0.5) == 21
+    with pytest.raises(ValueError):
+        f(0.0, 1024, 0.5)
