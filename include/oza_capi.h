@@ -144,6 +144,18 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
 
+/* C = A * B with A, B, C in HOST memory (row-major; pinned for overlap),
+ * synchronous.  Scheme II (fused path): the copies are pipelined with the
+ * compute in row chunks of A -- B is copied and sliced while A's chunks
+ * arrive, each chunk is sliced, multiplied and reconstructed as it lands,
+ * and its rows of C are copied back while the next chunk runs.  Other
+ * workspaces copy in, compute, copy out.  Device staging for A, B and C is
+ * allocated in the workspace on the first call.  timings->total_ms is the
+ * device time from the first copy to the last; the step fields are 0.
+ * Results are bit-identical to oza_gemm.
+ * Extension: the reference takes device buffers only (include/ozablas/ozablas.hpp:20,31). */
+oza_status_t oza_gemm_host(oza_ws_t ws, const double* A, const double* B, double* C, oza_timings_t* timings);
+
 /* ---- grouped Scheme II GEMM ------------------------------------------------ */
 /* Many independent row-major FP64 GEMMs C_i = A_i (M_i x K_i) * B_i (K_i x N_i),
  * each with its own slice count, run as one launch per stage: step 1 and 2

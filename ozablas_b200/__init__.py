@@ -26,7 +26,7 @@ __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
-    "autotune_slices", "GroupGemm", "Server", "slices_for_target",
+    "autotune_slices", "GroupGemm", "Server", "slices_for_target", "ozaki_gemm_host",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         "oza_ws_get_ptr": (I, [P, I, ctypes.POINTER(P)]),
         "oza_ws_get_info": (I, [P, ctypes.POINTER(_WsInfo)]),
         "oza_gemm": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
+        "oza_gemm_host": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
         "oza_ws_device_error": (I, [P, ctypes.POINTER(I)]),
         "oza_generate_matrix": (I, [I, I, ctypes.c_double, I, P]),
         "oza_scheme1_beta": (I, [S]),
@@ -467,6 +468,41 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def _host_ptr(x, shape, writable=False) -> int:
+    """Address of a C-contiguous float64 host array (numpy or CPU torch tensor)."""
+    if hasattr(x, "data_ptr"):
+        if x.is_cuda:
+            raise ValueError("host matrix expected (a CPU tensor or numpy array)")
+        if not x.is_contiguous() or str(x.dtype) != "torch.float64":
+            raise ValueError("host matrices must be contiguous float64")
+        if tuple(x.shape) != tuple(shape):
+            raise ValueError(f"shape {tuple(x.shape)} does not match {tuple(shape)}")
+        return int(x.data_ptr())
+    import numpy as np
+    if not isinstance(x, np.ndarray) or x.dtype != np.float64 or not x.flags["C_CONTIGUOUS"]:
+        raise ValueError("host matrices must be C-contiguous float64 numpy arrays or CPU tensors")
+    if writable and not x.flags["WRITEABLE"]:
+        raise ValueError("output array is read-only")
+    if tuple(x.shape) != tuple(shape):
+        raise ValueError(f"shape {tuple(x.shape)} does not match {tuple(shape)}")
+    return int(x.ctypes.data)
+
+
+def ozaki_gemm_host(ws, A, B, C, timings: OzaTimings | None = None) -> None:
+    """C = A * B with host matrices (pinned CPU tensors overlap the copies with
+    the compute), synchronous; bit-identical to the device-buffer call
+    (extension: oza_gemm_host)."""
+    M, N, K = ws.get_M(), ws.get_N(), ws.get_K()
+    t = _Timings() if timings is not None else None
+    _check(lib().oza_gemm_host(ws.handle, ctypes.c_void_p(_host_ptr(A, (M, K))),
+                               ctypes.c_void_p(_host_ptr(B, (K, N))),
+                               ctypes.c_void_p(_host_ptr(C, (M, N), writable=True)),
+                               ctypes.byref(t) if t is not None else None))
+    if timings is not None:
+        for f, _ in _Timings._fields_:
+            setattr(timings, f, float(getattr(t, f)))
 
 
 def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):

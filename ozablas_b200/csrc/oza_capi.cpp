@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -75,17 +76,60 @@ struct oza_workspace {
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     oza::PairList pairs{};
+    // oza_gemm_host: device staging of A, B, C, copy streams and chunk events,
+    // made on first use.
+    struct HostPipe {
+        double* dA = nullptr;
+        double* dB = nullptr;
+        double* dC = nullptr;
+        cudaStream_t cin = nullptr, cout = nullptr;
+        cudaEvent_t t0 = nullptr, t1 = nullptr, b_in = nullptr, out_done = nullptr;
+        cudaEvent_t a_in[8] = {}, done[8] = {};
+    } hp;
 };
 
 namespace {
 
 
 void ws_release(oza_workspace* ws) {
-    void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->coef, ws->err};
+    auto& h = ws->hp;
+    if (h.cin) cudaStreamSynchronize(h.cin);
+    if (h.cout) cudaStreamSynchronize(h.cout);
+    void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->coef, ws->err,
+                    h.dA, h.dB, h.dC};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (auto& e : ws->ev)
         if (e) cudaEventDestroy(e);
+    cudaEvent_t evs[] = {h.t0, h.t1, h.b_in, h.out_done};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    for (int i = 0; i < 8; ++i) {
+        if (h.a_in[i]) cudaEventDestroy(h.a_in[i]);
+        if (h.done[i]) cudaEventDestroy(h.done[i]);
+    }
+    if (h.cin) cudaStreamDestroy(h.cin);
+    if (h.cout) cudaStreamDestroy(h.cout);
+}
+
+cudaError_t host_pipe_init(oza_workspace* ws) {
+    auto& h = ws->hp;
+    if (h.dC) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&h.dA), ws->M * ws->K * sizeof(double) + 16);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&h.dB), ws->K * ws->N * sizeof(double) + 16);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h.cin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h.cout, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&h.t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&h.t1);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.b_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.out_done, cudaEventDisableTiming);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&h.a_in[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.done[i], cudaEventDisableTiming);
+    }
+    // dC last: its presence marks a complete set-up.
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&h.dC), ws->M * ws->N * sizeof(double) + 16);
+    return e;
 }
 
 }  // namespace
@@ -420,6 +464,101 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         OZA_CUDA_TRY(cudaMemcpy(&code, ws->err, sizeof(int), cudaMemcpyDeviceToHost), "CUDA: error word read");
         if (code) return fail(OZA_TIMEOUT, "OzaBLAS: a device-side wait expired (code %d)", code);
     }
+    return OZA_OK;
+}
+
+oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, double* hC, oza_timings_t* timings) {
+    if (!ws) return fail(OZA_INVALID_ARG, "oza_gemm_host: null workspace");
+    if (timings) std::memset(timings, 0, sizeof(*timings));
+    if (ws->M == 0 || ws->N == 0) return OZA_OK;
+    if (!hC || (ws->K && (!hA || !hB))) return fail(OZA_INVALID_ARG, "oza_gemm_host: null matrix pointer");
+    oza_executor* ex = ws->ex;
+    DeviceGuard g(ex->device);
+    if (!g.ok) return fail(OZA_CUDA_ERROR, "CUDA: Failed to set device %d", ex->device);
+    OZA_CUDA_TRY(host_pipe_init(ws), "oza_gemm_host: staging buffers");
+    auto& h = ws->hp;
+    cudaStream_t st = ex->stream;
+    const size_t M = ws->M, N = ws->N, K = ws->K;
+    OZA_CUDA_TRY(cudaEventRecord(h.t0, st), "CUDA: event record");
+
+    if (!ws->fused || K == 0) {
+        // Scheme I, the materialised path and K = 0: copy in, compute, copy out.
+        if (K) {
+            OZA_CUDA_TRY(cudaMemcpyAsync(h.dA, hA, M * K * sizeof(double), cudaMemcpyHostToDevice, st), "H2D A");
+            OZA_CUDA_TRY(cudaMemcpyAsync(h.dB, hB, K * N * sizeof(double), cudaMemcpyHostToDevice, st), "H2D B");
+        }
+        oza_status_t r = oza_gemm(ws, h.dA, h.dB, h.dC, nullptr);
+        if (r != OZA_OK) return r;
+        OZA_CUDA_TRY(cudaMemcpyAsync(hC, h.dC, M * N * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H C");
+    } else {
+        // Row-chunk pipeline: B is copied and sliced while A's chunks arrive;
+        // each A chunk is sliced, multiplied against all of B (its m-tiles
+        // only) and reconstructed, and its rows of C go back while the next
+        // chunk is computed.  Copies in and out run on their own streams.
+        const int offset = ws->k_param;
+        const size_t tile_m = ws->pair ? oza::kTileMPair : oza::kTileM;
+        const int mt_all = (int)(ws->Mp / tile_m);
+        const int R0 = mt_all < 8 ? mt_all : 8;
+        const int q = (mt_all + R0 - 1) / R0;   // m-tiles per chunk
+        const int R = (mt_all + q - 1) / q;
+        OZA_CUDA_TRY(cudaStreamWaitEvent(h.cin, h.t0, 0), "CUDA: stream wait");
+        OZA_CUDA_TRY(cudaStreamWaitEvent(h.cout, h.t0, 0), "CUDA: stream wait");
+        OZA_CUDA_TRY(cudaMemcpyAsync(h.dB, hB, K * N * sizeof(double), cudaMemcpyHostToDevice, h.cin), "H2D B");
+        OZA_CUDA_TRY(cudaEventRecord(h.b_in, h.cin), "CUDA: event record");
+        OZA_CUDA_TRY(cudaStreamWaitEvent(st, h.b_in, 0), "CUDA: stream wait");
+        OZA_CUDA_TRY(oza::launch_stats_cols(h.dB, K, N, ws->colmax, ex->sms, st), "step1 cols");
+        OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, h.dB, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
+                                            ws->bplanes, ws->Np, ws->Kp, st),
+                     "step2 cols");
+        for (int c = 0; c < R; ++c) {
+            const size_t r0 = (size_t)c * q * tile_m;
+            const size_t rows_p = std::min((size_t)q * tile_m, ws->Mp - r0);
+            const size_t rows = std::min(M, r0 + rows_p) - r0;   // >= 1: chunks start on tile boundaries below Mp
+            OZA_CUDA_TRY(cudaMemcpyAsync(h.dA + r0 * K, hA + r0 * K, rows * K * sizeof(double),
+                                         cudaMemcpyHostToDevice, h.cin),
+                         "H2D A chunk");
+            OZA_CUDA_TRY(cudaEventRecord(h.a_in[c], h.cin), "CUDA: event record");
+            OZA_CUDA_TRY(cudaStreamWaitEvent(st, h.a_in[c], 0), "CUDA: stream wait");
+            OZA_CUDA_TRY(oza::launch_stats_rows(h.dA + r0 * K, rows, K, offset, ws->shiftA + r0, ex->sms, st),
+                         "step1 rows");
+            OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, h.dA + r0 * K, rows, K, ws->shiftA + r0, ws->S, ws->beta,
+                                                offset, ws->aplanes + r0 * ws->Kp, rows_p, ws->Kp, ex->sms, st,
+                                                ws->Mp),
+                         "step2 rows");
+            oza::GemmPlan plan;
+            plan.a_planes = ws->aplanes;
+            plan.b_planes = ws->bplanes;
+            plan.planes = ws->S;
+            plan.Mp = ws->Mp;
+            plan.Np = ws->Np;
+            plan.Kp = ws->Kp;
+            plan.pairs = ws->pairs;
+            plan.err = ws->err;
+            plan.sms = ex->sms;
+            plan.pair = ws->pair;
+            plan.ctc = nullptr;
+            plan.coef = ws->coef;
+            plan.m_tile_begin = c * q;
+            plan.m_tile_count = std::min(q, mt_all - c * q);
+            OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
+            OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->shiftA + r0,
+                                              ws->shiftB, h.dC + r0 * N, ex->sms, st),
+                         "step4 crt");
+            OZA_CUDA_TRY(cudaEventRecord(h.done[c], st), "CUDA: event record");
+            OZA_CUDA_TRY(cudaStreamWaitEvent(h.cout, h.done[c], 0), "CUDA: stream wait");
+            OZA_CUDA_TRY(cudaMemcpyAsync(hC + r0 * N, h.dC + r0 * N, rows * N * sizeof(double),
+                                         cudaMemcpyDeviceToHost, h.cout),
+                         "D2H C chunk");
+        }
+        OZA_CUDA_TRY(cudaEventRecord(h.out_done, h.cout), "CUDA: event record");
+        OZA_CUDA_TRY(cudaStreamWaitEvent(st, h.out_done, 0), "CUDA: stream wait");
+    }
+    OZA_CUDA_TRY(cudaEventRecord(h.t1, st), "CUDA: event record");
+    OZA_CUDA_TRY(cudaEventSynchronize(h.t1), "CUDA: event synchronize");
+    if (timings) cudaEventElapsedTime(&timings->total_ms, h.t0, h.t1);
+    int code = 0;
+    OZA_CUDA_TRY(cudaMemcpy(&code, ws->err, sizeof(int), cudaMemcpyDeviceToHost), "CUDA: error word read");
+    if (code) return fail(OZA_TIMEOUT, "OzaBLAS: a device-side wait expired (code %d)", code);
     return OZA_OK;
 }
 

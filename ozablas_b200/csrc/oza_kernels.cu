@@ -493,10 +493,10 @@ __device__ __forceinline__ void slice_rows_chunk(const double* __restrict__ A, l
 template <int SCHEME, int SC, bool WIDE>
 __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_rows(
     const double* __restrict__ A, long long rows, long long cols, const int32_t* __restrict__ shift, int S, int beta,
-    int8_t* __restrict__ out, long long rows_p, long long cols_p) {
+    int8_t* __restrict__ out, long long rows_p, long long cols_p, long long plane_rows) {
     constexpr int E = SCHEME == 2 ? 8 : 16;
     const long long total = rows_p * (cols_p / E);
-    const size_t plane = (size_t)rows_p * (size_t)cols_p;
+    const size_t plane = (size_t)plane_rows * (size_t)cols_p;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
          id += (long long)gridDim.x * blockDim.x)
         slice_rows_chunk<SCHEME, SC, WIDE>(A, rows, cols, shift, S, beta, out, cols_p, plane, id);
@@ -714,6 +714,7 @@ constexpr int kEpiCoef = 1;
 
 struct GemmArgs {
     int m_tiles, n_tiles, k_blocks, total_tiles, groups;
+    int mt0;                      // first m-tile (row-chunked calls)
     int band;                     // m-tiles per rasterisation band
     long long Mp, Np;
     int* err;
@@ -731,7 +732,7 @@ __device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, i
     const int tb = t - b * per_band;
     const int rows = min(a.band, a.m_tiles - b * a.band);
     nt = tb / rows;
-    mt = b * a.band + (tb - nt * rows);
+    mt = a.mt0 + b * a.band + (tb - nt * rows);
 }
 
 // One work unit's epilogue for one warp: 32 TMEM lanes (rows) x 128 columns
@@ -1522,13 +1523,14 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift, int S,
                               int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
-                              cudaStream_t st) {
+                              cudaStream_t st, size_t plane_rows) {
     long long chunks = (long long)rows_p * (long long)(cols_p / (scheme == 2 ? 8 : 16));
     if (chunks == 0) return cudaSuccess;
     const int grid = grid_for(chunks, 256, sms);
     const long long R = (long long)rows, C = (long long)cols, RP = (long long)rows_p, CP = (long long)cols_p;
+    const long long PR = plane_rows ? (long long)plane_rows : RP;
     if (scheme == 1) {
-        k_slice_rows<1, 0, false><<<grid, 256, 0, st>>>(A, R, C, shift, S, beta, out, RP, CP);
+        k_slice_rows<1, 0, false><<<grid, 256, 0, st>>>(A, R, C, shift, S, beta, out, RP, CP, PR);
         return cudaGetLastError();
     }
     const bool wide = k_param > 62;
@@ -1536,8 +1538,8 @@ cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t c
     switch (S) {
 #define OZA_CASE(n)                                                                                   \
     case n:                                                                                           \
-        if (wide) k_slice_rows<2, n, (n >= 17)><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP); \
-        else k_slice_rows<2, n, false><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP);         \
+        if (wide) k_slice_rows<2, n, (n >= 17)><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP, PR); \
+        else k_slice_rows<2, n, false><<<grid, 256, 0, st>>>(A, R, C, shift, n, 0, out, RP, CP, PR);         \
         break;
         OZA_FOR_EACH_S(OZA_CASE)
 #undef OZA_CASE
@@ -1605,7 +1607,11 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, p.pair ? 128 : kTileN))
         return cudaErrorInvalidValue;
     GemmArgs a{};
-    a.m_tiles = (int)(p.Mp / tile_m);
+    const int all_m_tiles = (int)(p.Mp / tile_m);
+    if (p.m_tile_begin < 0 || p.m_tile_count < 0 || p.m_tile_begin + p.m_tile_count > all_m_tiles)
+        return cudaErrorInvalidValue;
+    a.mt0 = p.m_tile_begin;
+    a.m_tiles = p.m_tile_count ? p.m_tile_count : all_m_tiles - p.m_tile_begin;
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
     a.total_tiles = a.m_tiles * a.n_tiles;

@@ -42,9 +42,11 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 // Step 2.  scheme 1: slices with width beta from shifts (offset 0);
 // scheme 2: symmetric residues of rint(ldexp(x, shift)).
 // Rows: A (rows x cols, row-major) -> out[s][rows_p][cols_p].
+// plane_rows: rows between planes of `out` (0: rows_p), so a row chunk can be
+// sliced into its place in full-size planes.
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift,
                               int S, int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
-                              cudaStream_t st);
+                              cudaStream_t st, size_t plane_rows = 0);
 // Columns: B (K x N, row-major) -> out[s][Np][Kp] (transposed, K-major); also
 // writes shift[n] = offset - max exponent of column n.
 cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
@@ -64,6 +66,8 @@ struct GemmPlan {
     // epilogue output: INT32 group planes, or (Scheme II) CRT coefficient bytes
     int32_t* ctc;             // [groups][Mp][Np], used when coef == nullptr
     uint8_t* coef;            // [S][Mp][Np]
+    int m_tile_begin = 0;     // restrict the launch to m-tiles [begin, begin + count) (count 0: to the end)
+    int m_tile_count = 0;
 };
 cudaError_t launch_gemm_i8(const GemmPlan& plan, cudaStream_t st);
 
