@@ -144,6 +144,36 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
 
+/* ---- GEMM tuning ------------------------------------------------------------ */
+/* Step-3 kernel configuration of a workspace (0 fields: library defaults).
+ *   pair_stages  TMA pipeline depth of the CTA-pair kernel, 4..7 (default 6)
+ *   band         m-tiles per rasterisation band (default 16)
+ *   one_cta      1: one-CTA 128 x 256 tiles instead of CTA-pair 256 x 256 tiles
+ *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
+ *   overlap_chunks  Scheme II fused path, calls without timings: >= 2 splits
+ *                the GEMM into that many row chunks and overlaps A's slicing
+ *                and each chunk's reconstruction with the GEMM on other
+ *                streams; 1: the four steps run one after another; 0: 4
+ *                chunks from 32 row tiles, 2 from 4, else 1.  Calls with
+ *                timings always run the steps one after another.
+ * Results do not depend on the configuration (bit-identical).
+ * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
+typedef struct {
+    int pair_stages;
+    int band;
+    int one_cta;
+    int wait_hint_ns;
+    int overlap_chunks;
+} oza_gemm_config_t;
+
+oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg); /* NULL: defaults */
+oza_status_t oza_ws_get_gemm_config(oza_ws_t ws, oza_gemm_config_t* cfg);
+/* Times every configuration on this workspace with these device inputs
+ * (step 3 device time, best of 2 after a warm-up), keeps the fastest on the
+ * workspace and returns it.  C is overwritten. */
+oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, double* C, oza_gemm_config_t* best,
+                               float* best_step3_ms);
+
 /* C = A * B with A, B, C in HOST memory (row-major; pinned for overlap),
  * synchronous.  Scheme II (fused path): the copies are pipelined with the
  * compute in row chunks of A -- B is copied and sliced while A's chunks

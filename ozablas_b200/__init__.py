@@ -61,6 +61,11 @@ class _WsInfo(ctypes.Structure):
                 ("flags", ctypes.c_uint), ("bytes", ctypes.c_size_t)]
 
 
+class _GemmConfig(ctypes.Structure):
+    _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("one_cta", ctypes.c_int),
+                ("wait_hint_ns", ctypes.c_int), ("overlap_chunks", ctypes.c_int)]
+
+
 class _GroupInfo(ctypes.Structure):
     _fields_ = [("count", ctypes.c_size_t), ("units", ctypes.c_size_t), ("bytes", ctypes.c_size_t),
                 ("launches", ctypes.c_int), ("graph", ctypes.c_int)]
@@ -124,6 +129,9 @@ def lib() -> ctypes.CDLL:
         "oza_ws_get_info": (I, [P, ctypes.POINTER(_WsInfo)]),
         "oza_gemm": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
         "oza_gemm_host": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
+        "oza_ws_set_gemm_config": (I, [P, ctypes.POINTER(_GemmConfig)]),
+        "oza_ws_get_gemm_config": (I, [P, ctypes.POINTER(_GemmConfig)]),
+        "oza_autotune_gemm": (I, [P, P, P, P, ctypes.POINTER(_GemmConfig), ctypes.POINTER(ctypes.c_float)]),
         "oza_ws_device_error": (I, [P, ctypes.POINTER(I)]),
         "oza_generate_matrix": (I, [I, I, ctypes.c_double, I, P]),
         "oza_scheme1_beta": (I, [S]),
@@ -289,6 +297,26 @@ class _Workspace:
         c = ctypes.c_int()
         _check(lib().oza_ws_device_error(self._h, ctypes.byref(c)))
         return c.value
+
+    def set_gemm_config(self, pair_stages: int = 0, band: int = 0, one_cta: bool = False,
+                        wait_hint_ns: int = 0, overlap_chunks: int = 0) -> None:
+        """Step-3 kernel configuration (0: defaults); results are unaffected."""
+        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(one_cta)), int(wait_hint_ns), int(overlap_chunks))
+        _check(lib().oza_ws_set_gemm_config(self._h, ctypes.byref(cfg)))
+
+    def get_gemm_config(self) -> dict:
+        cfg = _GemmConfig()
+        _check(lib().oza_ws_get_gemm_config(self._h, ctypes.byref(cfg)))
+        return {f: getattr(cfg, f) for f, _ in _GemmConfig._fields_}
+
+    def autotune_gemm(self, A, B, C):
+        """Time every step-3 configuration on these inputs, keep the fastest;
+        returns (config dict, step-3 ms).  C is overwritten."""
+        cfg = _GemmConfig()
+        ms = ctypes.c_float()
+        _check(lib().oza_autotune_gemm(self._h, ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)),
+                                       ctypes.c_void_p(_ptr(C)), ctypes.byref(cfg), ctypes.byref(ms)))
+        return {f: getattr(cfg, f) for f, _ in _GemmConfig._fields_}, ms.value
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -715,6 +715,7 @@ constexpr int kEpiCoef = 1;
 struct GemmArgs {
     int m_tiles, n_tiles, k_blocks, total_tiles, groups;
     int mt0;                      // first m-tile (row-chunked calls)
+    uint32_t wait_hint;           // mbarrier suspend-time hint in ns (0: poll)
     int band;                     // m-tiles per rasterisation band
     long long Mp, Np;
     int* err;
@@ -828,6 +829,7 @@ struct GroupGemmProblem {
 struct GroupGemmArgs {
     const int4* units;
     int total_units;
+    uint32_t wait_hint;
     const CUtensorMap* maps;   // [2 * problems]: A planes, then B^T planes
     const GroupGemmProblem* probs;
     int* err;
@@ -861,7 +863,7 @@ struct GroupUnits {
 // TMEM accumulators, warps 2-9 drain the other accumulator through the
 // epilogue.  CTA c takes units c, c + grid, ...  Every wait is bounded.
 template <int EPI, class Units>
-__device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
+__device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_t hint) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -918,7 +920,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
                 const int brow = (int)(src.b_plane(p) * x.Np + (long long)x.nt * kTileN);
                 for (int kb = 0; kb < x.k_blocks; ++kb) {
                     int w = 1;
-                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, err);
+                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, err, hint);
                     ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
                     if (!ok) break;
                     if (lane == 0) {
@@ -957,7 +959,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
             const int acc = local & 1;
             const uint32_t acc_phase = (local >> 1) & 1;
             int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, err);
+            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, err, hint);
             ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
             if (!ok) break;
             tc_fence_after();
@@ -966,7 +968,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
             for (int p = x.p0; p < x.p1 && ok; ++p) {
                 for (int kb = 0; kb < x.k_blocks; ++kb) {
                     w = 1;
-                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, err);
+                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, err, hint);
                     ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
                     if (!ok) break;
                     tc_fence_after();
@@ -1013,7 +1015,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err) {
             const int acc = local & 1;
             const uint32_t acc_phase = (local >> 1) & 1;
             int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, err);
+            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, err, hint);
             if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
                 ok = false;
                 continue;
@@ -1041,13 +1043,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const __grid_constant__ PairList pairs, const __grid_constant__ GemmArgs args) {
     const SingleUnits src{&tmA, &tmB, &pairs, &args};
-    gemm_i8_body<EPI>(src, args.err);
+    gemm_i8_body<EPI>(src, args.err, args.wait_hint);
 }
 
 // Grouped Scheme II GEMM over an explicit unit list (coefficient epilogue).
 __global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_constant__ GroupGemmArgs g) {
     const GroupUnits src{&g};
-    gemm_i8_body<kEpiCoef>(src, g.err);
+    gemm_i8_body<kEpiCoef>(src, g.err, g.wait_hint);
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,16 +1067,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_
 // are counted on its full barriers; MMA commits arrive on both CTAs'
 // barriers; both CTAs' epilogue warps release the accumulator on the even
 // CTA's acc_empty barrier.  No TMA multicast is used.
-constexpr int kPairStages = 6;
 constexpr int kPairTileM = 256;                   // rows of C per CTA pair
 constexpr int kPairABytes = 128 * kTileK;         // this CTA's 128 rows of A
 constexpr int kPairBBytes = 128 * kTileK;         // this CTA's half of B^T
-constexpr int kPairSmem = kPairStages * (kPairABytes + kPairBBytes) + 1024 + 256;
+constexpr int kPairStagesDefault = 6;
+template <int STAGES>
+constexpr int pair_smem() { return STAGES * (kPairABytes + kPairBBytes) + 1024 + 256; }
+static_assert(pair_smem<7>() <= 232448, "7 pair stages must fit in 227 KB of shared memory");
 
-template <int EPI>
+template <int EPI, int kPairStages>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     k_gemm_i8_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const __grid_constant__ PairList pairs, const GemmArgs args) {
+    const uint32_t hint = args.wait_hint;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -1131,7 +1136,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
                 const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN + rank * 128);
                 for (int kb = 0; kb < args.k_blocks; ++kb) {
                     int w = 1;
-                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err);
+                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err, hint);
                     ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
                     if (!ok) break;
                     if (lane == 0) {
@@ -1170,7 +1175,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
                 const int acc = local & 1;
                 const uint32_t acc_phase = (local >> 1) & 1;
                 int w = 1;
-                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err);
+                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err, hint);
                 ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
                 if (!ok) break;
                 tc_fence_after();
@@ -1179,7 +1184,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
                 for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
                     for (int kb = 0; kb < args.k_blocks; ++kb) {
                         w = 1;
-                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err);
+                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err, hint);
                         ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
                         if (!ok) break;
                         tc_fence_after();
@@ -1228,7 +1233,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
             const int acc = local & 1;
             const uint32_t acc_phase = (local >> 1) & 1;
             int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err);
+            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err, hint);
             if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
                 ok = false;
                 continue;
@@ -1586,25 +1591,39 @@ static cudaError_t gemm_launch(const CUtensorMap& tmA, const CUtensorMap& tmB, c
     return cudaGetLastError();
 }
 
-template <int EPI>
-static cudaError_t gemm_launch_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
-                                    const GemmArgs& a, int grid, cudaStream_t st) {
+template <int EPI, int STAGES>
+static cudaError_t gemm_launch_pair_s(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
+                                      const GemmArgs& a, int grid, cudaStream_t st) {
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_gemm_i8_pair<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem);
+        attr = cudaFuncSetAttribute(k_gemm_i8_pair<EPI, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    pair_smem<STAGES>());
     });
     if (attr != cudaSuccess) return attr;
-    k_gemm_i8_pair<EPI><<<grid, kGemmThreads, kPairSmem, st>>>(tmA, tmB, pairs, a);
+    k_gemm_i8_pair<EPI, STAGES><<<grid, kGemmThreads, pair_smem<STAGES>(), st>>>(tmA, tmB, pairs, a);
     return cudaGetLastError();
 }
 
+template <int EPI>
+static cudaError_t gemm_launch_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
+                                    const GemmArgs& a, int grid, int stages, cudaStream_t st) {
+    switch (stages) {
+        case 4: return gemm_launch_pair_s<EPI, 4>(tmA, tmB, pairs, a, grid, st);
+        case 5: return gemm_launch_pair_s<EPI, 5>(tmA, tmB, pairs, a, grid, st);
+        case 6: return gemm_launch_pair_s<EPI, 6>(tmA, tmB, pairs, a, grid, st);
+        case 7: return gemm_launch_pair_s<EPI, 7>(tmA, tmB, pairs, a, grid, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
-    const int tile_m = p.pair ? kPairTileM : kTileM;
+    const bool pair = p.pair && !p.one_cta;
+    const int tile_m = pair ? kPairTileM : kTileM;
     if (p.Mp % tile_m != 0) return cudaErrorInvalidValue;
     CUtensorMap tmA, tmB;
     if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, 128)) return cudaErrorInvalidValue;
-    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, p.pair ? 128 : kTileN))
+    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, pair ? 128 : kTileN))
         return cudaErrorInvalidValue;
     GemmArgs a{};
     const int all_m_tiles = (int)(p.Mp / tile_m);
@@ -1615,7 +1634,8 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
     a.total_tiles = a.m_tiles * a.n_tiles;
-    const int band = 16;   // measured: pair bands of 8 / 16 / 32 m-tiles read 9.5 / 7.0 / 11.0 GB at 8192^3 S=16
+    // Default band measured: pair bands of 8 / 16 / 32 m-tiles read 9.5 / 7.0 / 11.0 GB at 8192^3 S=16.
+    const int band = p.band > 0 ? p.band : 16;
     a.band = a.m_tiles < band ? a.m_tiles : band;
     a.groups = p.pairs.num_groups;
     a.Mp = (long long)p.Mp;
@@ -1624,13 +1644,15 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.ctc = p.ctc;
     a.coef = p.coef;
     a.S = p.planes;
+    a.wait_hint = p.wait_hint_ns;
     const long long units = (long long)a.total_tiles * a.groups;
     if (units == 0) return cudaSuccess;
-    if (p.pair) {
+    if (pair) {
         const long long pairs_max = p.sms / 2;
         const int grid = 2 * (int)(units < pairs_max ? units : pairs_max);
-        return p.coef ? gemm_launch_pair<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
-                      : gemm_launch_pair<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);
+        const int stages = p.stages > 0 ? p.stages : kPairStagesDefault;
+        return p.coef ? gemm_launch_pair<kEpiCoef>(tmA, tmB, p.pairs, a, grid, stages, st)
+                      : gemm_launch_pair<kEpiI32>(tmA, tmB, p.pairs, a, grid, stages, st);
     }
     const int grid = (int)(units < p.sms ? units : p.sms);
     return p.coef ? gemm_launch<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
@@ -1782,9 +1804,17 @@ cudaError_t group_plan_build(const GroupProblem* in, int count, int* err, GroupP
     // Longest units first (cost ~ k_blocks): CTA c takes units c, c + grid, ...,
     // so each round of `grid` units has near-equal cost.  Stable, so units of
     // one problem and modulus stay together for L2 reuse.
-    std::stable_sort(units.begin(), units.end(), [&](const int4& x, const int4& y) {
-        return gprobs[x.x].k_blocks > gprobs[y.x].k_blocks;
-    });
+    {
+        // Counting sort on k_blocks, descending, stable.
+        int maxkb = 0;
+        for (const auto& gpr : gprobs) maxkb = std::max(maxkb, gpr.k_blocks);
+        std::vector<size_t> pos(maxkb + 2, 0);
+        for (const int4& u : units) ++pos[maxkb - gprobs[u.x].k_blocks + 1];
+        for (int b = 1; b <= maxkb + 1; ++b) pos[b] += pos[b - 1];
+        std::vector<int4> sorted(units.size());
+        for (const int4& u : units) sorted[pos[maxkb - gprobs[u.x].k_blocks]++] = u;
+        units.swap(sorted);
+    }
 
     // Per-stage block maps; the templated stages split by (S, wide) class.
     auto tiles_of = [&](const GroupProblemDev& d, int stage) -> long long {

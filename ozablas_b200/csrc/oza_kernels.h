@@ -68,6 +68,12 @@ struct GemmPlan {
     uint8_t* coef;            // [S][Mp][Np]
     int m_tile_begin = 0;     // restrict the launch to m-tiles [begin, begin + count) (count 0: to the end)
     int m_tile_count = 0;
+    // Tuning (0: defaults): pair-kernel pipeline stages (4..7), m-tiles per
+    // rasterisation band, and the one-CTA kernel in place of the pair kernel.
+    int stages = 0;
+    int band = 0;
+    bool one_cta = false;
+    uint32_t wait_hint_ns = 0;   // mbarrier suspend-time hint of the kernel's waits (0: poll)
 };
 cudaError_t launch_gemm_i8(const GemmPlan& plan, cudaStream_t st);
 

@@ -155,6 +155,7 @@ struct oza_server {
     std::unordered_map<uint64_t, Request*> reqs;
     uint64_t next_id = 1;
     bool stop = false;
+    bool kick = false;                                // new work or a finished batch
     bool failed = false;
     std::string fail_msg;
     oza_server_stats_t st{};
@@ -167,6 +168,15 @@ struct oza_server {
     void run();
     bool poll();
     bool launch();
+    // Runs on the CUDA callback thread: no CUDA calls.
+    static void CUDART_CB batch_done(void* p) {
+        auto* s = static_cast<oza_server*>(p);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->kick = true;
+        }
+        s->cv_work.notify_one();
+    }
 };
 
 bool oza_server::poll() {
@@ -315,6 +325,9 @@ bool oza_server::launch() {
     if (e == cudaSuccess) e = oza::group_plan_launch(plan, colmax, ncol, ex->sms, sl->st, nullptr);
     if (e == cudaSuccess) e = cudaMemcpyAsync(sl->pinned, err, sizeof(int), cudaMemcpyDeviceToHost, sl->st);
     if (e == cudaSuccess) e = cudaEventRecord(sl->done, sl->st);
+    // Wake the scheduler as soon as the batch is done (after the event, so the
+    // scheduler then finds it complete).
+    if (e == cudaSuccess) e = cudaLaunchHostFunc(sl->st, &oza_server::batch_done, this);
     sl->plan = plan;
     sl->reqs = batch;
     sl->busy = true;
@@ -347,18 +360,20 @@ bool oza_server::launch() {
 void oza_server::run() {
     cudaSetDevice(ex->device);
     for (;;) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            kick = false;
+        }
         bool progressed = poll();
         while (launch()) progressed = true;
         bool idle = true;
         for (const Slot& s : slots) idle = idle && !s.busy;
         std::unique_lock<std::mutex> lk(mu);
         if (stop && queue.empty() && idle) break;
-        if (!progressed) {
-            // Busy slots are polled every 50 us; an idle server sleeps until a
-            // submission arrives.
-            if (idle && queue.empty() && !stop) cv_work.wait(lk);
-            else cv_work.wait_for(lk, std::chrono::microseconds(50));
-        }
+        if (progressed) continue;
+        // Submissions and finished batches kick the loop; the timeout is only
+        // a safety net.
+        cv_work.wait_for(lk, std::chrono::milliseconds(idle ? 100 : 2), [this] { return kick || stop; });
     }
 }
 
@@ -443,6 +458,7 @@ oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, con
             return sfail(OZA_INVALID_ARG, "oza_server_submit: server is shutting down");
         }
         r->id = s->next_id++;
+        s->kick = true;
         r->stats.submit_s = s->now();
         r->stats.slices = slices;
         r->stats.workspace_bytes = bytes;
@@ -489,6 +505,7 @@ oza_status_t oza_server_destroy(oza_server_t s) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
+        s->kick = true;
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();

@@ -159,3 +159,36 @@ def test_scheme2_fused_edge_cases(executor):
     for S in (8, 19):
         got = run_pipeline(oz, executor, 2, A, B, S, materialize=False)
         _check_all(got, Oracle.scheme2(A, B, S))
+
+
+@pytest.mark.parametrize("scheme,S", [(2, 16), (1, 5)])
+def test_gemm_configurations_are_bit_identical(executor, scheme, S):
+    """Every step-3 configuration (pipeline depth, band, one-CTA vs pair
+    tiles) gives the same bits; the autotuner keeps one of them."""
+    import torch
+    import ozablas_b200 as oz
+    M, N, K = 700, 520, 900
+    A = torch.from_numpy(oz.generate_matrix(M, K, 1.0, 1)).cuda()
+    B = torch.from_numpy(oz.generate_matrix(K, N, 1.0, 2)).cuda()
+    W = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(executor, M, N, K, S)
+    gemm = oz.ozaki_scheme2_gemm if scheme == 2 else oz.ozaki_scheme1_gemm
+    ref = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    gemm(W, A, B, ref)
+    for stages in (4, 5, 6, 7):
+        for band, one in ((8, False), (32, False), (16, True)):
+            W.set_gemm_config(stages, band, one)
+            C = torch.empty_like(ref)
+            gemm(W, A, B, C)
+            assert torch.equal(C.view(torch.int64), ref.view(torch.int64)), (stages, band, one)
+    if scheme == 2:
+        for chunks in (1, 2, 3, 16):   # sequential and overlapped stages: same bits
+            W.set_gemm_config(overlap_chunks=chunks)
+            for _ in range(2):
+                C = torch.full_like(ref, float("nan"))
+                gemm(W, A, B, C)
+                assert torch.equal(C.view(torch.int64), ref.view(torch.int64)), chunks
+    W.set_gemm_config()
+    cfg, ms = W.autotune_gemm(A, B, torch.empty_like(ref))
+    assert ms > 0 and W.get_gemm_config() == cfg
+    with pytest.raises(ValueError):
+        W.set_gemm_config(9, 16, False)
