@@ -150,12 +150,6 @@ oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t
  *   band         m-tiles per rasterisation band (default 16)
  *   one_cta      1: one-CTA 128 x 256 tiles instead of CTA-pair 256 x 256 tiles
  *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
- *   overlap_chunks  Scheme II fused path, calls without timings: >= 2 splits
- *                the GEMM into that many row chunks and overlaps A's slicing
- *                and each chunk's reconstruction with the GEMM on other
- *                streams; 1: the four steps run one after another; 0: 4
- *                chunks from 32 row tiles, 2 from 4, else 1.  Calls with
- *                timings always run the steps one after another.
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
 typedef struct {
@@ -163,7 +157,6 @@ typedef struct {
     int band;
     int one_cta;
     int wait_hint_ns;
-    int overlap_chunks;
 } oza_gemm_config_t;
 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg); /* NULL: defaults */

@@ -63,7 +63,7 @@ class _WsInfo(ctypes.Structure):
 
 class _GemmConfig(ctypes.Structure):
     _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("one_cta", ctypes.c_int),
-                ("wait_hint_ns", ctypes.c_int), ("overlap_chunks", ctypes.c_int)]
+                ("wait_hint_ns", ctypes.c_int)]
 
 
 class _GroupInfo(ctypes.Structure):
@@ -299,9 +299,9 @@ class _Workspace:
         return c.value
 
     def set_gemm_config(self, pair_stages: int = 0, band: int = 0, one_cta: bool = False,
-                        wait_hint_ns: int = 0, overlap_chunks: int = 0) -> None:
+                        wait_hint_ns: int = 0) -> None:
         """Step-3 kernel configuration (0: defaults); results are unaffected."""
-        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(one_cta)), int(wait_hint_ns), int(overlap_chunks))
+        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(one_cta)), int(wait_hint_ns))
         _check(lib().oza_ws_set_gemm_config(self._h, ctypes.byref(cfg)))
 
     def get_gemm_config(self) -> dict:

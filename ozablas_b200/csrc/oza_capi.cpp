@@ -77,7 +77,7 @@ struct oza_workspace {
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     oza::PairList pairs{};
-    oza_gemm_config_t cfg{0, 0, 0, 0, 0};  // GEMM tuning (0: library defaults)
+    oza_gemm_config_t cfg{0, 0, 0, 0};  // GEMM tuning (0: library defaults)
     // oza_gemm_host: device staging of A, B, C, copy streams and chunk events,
     // made on first use.
     struct HostPipe {
@@ -88,12 +88,6 @@ struct oza_workspace {
         cudaEvent_t t0 = nullptr, t1 = nullptr, b_in = nullptr, out_done = nullptr;
         cudaEvent_t a_in[8] = {}, done[8] = {};
     } hp;
-    // Overlapped device path: slicer and reconstruction streams, chunk events.
-    struct Overlap {
-        cudaStream_t s_slice = nullptr, s_crt = nullptr;
-        cudaEvent_t start = nullptr, b_done = nullptr, end = nullptr;
-        cudaEvent_t a_done[16] = {}, g_done[16] = {};
-    } ov;
 };
 
 namespace {
@@ -118,106 +112,8 @@ void ws_release(oza_workspace* ws) {
     }
     if (h.cin) cudaStreamDestroy(h.cin);
     if (h.cout) cudaStreamDestroy(h.cout);
-    auto& o = ws->ov;
-    if (o.s_slice) cudaStreamSynchronize(o.s_slice);
-    if (o.s_crt) cudaStreamSynchronize(o.s_crt);
-    cudaEvent_t oevs[] = {o.start, o.b_done, o.end};
-    for (cudaEvent_t e : oevs)
-        if (e) cudaEventDestroy(e);
-    for (int i = 0; i < 16; ++i) {
-        if (o.a_done[i]) cudaEventDestroy(o.a_done[i]);
-        if (o.g_done[i]) cudaEventDestroy(o.g_done[i]);
-    }
-    if (o.s_slice) cudaStreamDestroy(o.s_slice);
-    if (o.s_crt) cudaStreamDestroy(o.s_crt);
 }
 
-cudaError_t overlap_init(oza_workspace* ws) {
-    auto& o = ws->ov;
-    if (o.end) return cudaSuccess;
-    cudaError_t e = cudaStreamCreateWithFlags(&o.s_slice, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&o.s_crt, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.start, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.b_done, cudaEventDisableTiming);
-    for (int i = 0; i < 16 && e == cudaSuccess; ++i) {
-        e = cudaEventCreateWithFlags(&o.a_done[i], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.g_done[i], cudaEventDisableTiming);
-    }
-    // `end` last: its presence marks a complete set-up.
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.end, cudaEventDisableTiming);
-    return e;
-}
-
-// Scheme II fused path with stages overlapped across streams: B is sliced on
-// the executor's stream while A's row chunks are sliced on a second one; the
-// GEMM runs chunk by chunk on the executor's stream; each chunk's CRT runs on
-// a third stream while the next chunk's GEMM runs.  Same kernels, same
-// results as the sequential path.
-oza_status_t gemm_overlapped(oza_workspace* ws, const double* A, const double* B, double* C, int chunks) {
-    oza_executor* ex = ws->ex;
-    auto& o = ws->ov;
-    cudaStream_t st = ex->stream;
-    const size_t M = ws->M, N = ws->N, K = ws->K;
-    const int offset = ws->k_param;
-    const bool pair = ws->pair && !ws->cfg.one_cta;
-    const size_t tile_m = pair ? oza::kTileMPair : oza::kTileM;
-    const int mt_all = (int)(ws->Mp / tile_m);
-    const int R0 = std::min(std::min(chunks, 16), mt_all);
-    const int q = (mt_all + R0 - 1) / R0;
-    const int R = (mt_all + q - 1) / q;
-    OZA_CUDA_TRY(cudaEventRecord(o.start, st), "CUDA: event record");
-    OZA_CUDA_TRY(cudaStreamWaitEvent(o.s_slice, o.start, 0), "CUDA: stream wait");
-    OZA_CUDA_TRY(cudaStreamWaitEvent(o.s_crt, o.start, 0), "CUDA: stream wait");
-    OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, st), "step1 cols");
-    OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
-                                        ws->bplanes, ws->Np, ws->Kp, st),
-                 "step2 cols");
-    for (int c = 0; c < R; ++c) {
-        const size_t r0 = (size_t)c * q * tile_m;
-        const size_t rows_p = std::min((size_t)q * tile_m, ws->Mp - r0);
-        const size_t rows = std::min(M, r0 + rows_p) - r0;
-        OZA_CUDA_TRY(oza::launch_stats_rows(A + r0 * K, rows, K, offset, ws->shiftA + r0, ex->sms, o.s_slice),
-                     "step1 rows");
-        OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A + r0 * K, rows, K, ws->shiftA + r0, ws->S, ws->beta, offset,
-                                            ws->aplanes + r0 * ws->Kp, rows_p, ws->Kp, ex->sms, o.s_slice, ws->Mp),
-                     "step2 rows");
-        OZA_CUDA_TRY(cudaEventRecord(o.a_done[c], o.s_slice), "CUDA: event record");
-    }
-    for (int c = 0; c < R; ++c) {
-        const size_t r0 = (size_t)c * q * tile_m;
-        const size_t rows_p = std::min((size_t)q * tile_m, ws->Mp - r0);
-        const size_t rows = std::min(M, r0 + rows_p) - r0;
-        OZA_CUDA_TRY(cudaStreamWaitEvent(st, o.a_done[c], 0), "CUDA: stream wait");
-        oza::GemmPlan plan;
-        plan.a_planes = ws->aplanes;
-        plan.b_planes = ws->bplanes;
-        plan.planes = ws->S;
-        plan.Mp = ws->Mp;
-        plan.Np = ws->Np;
-        plan.Kp = ws->Kp;
-        plan.pairs = ws->pairs;
-        plan.err = ws->err;
-        plan.sms = ex->sms;
-        plan.pair = ws->pair;
-        plan.ctc = nullptr;
-        plan.coef = ws->coef;
-        plan.m_tile_begin = c * q;
-        plan.m_tile_count = std::min(q, mt_all - c * q);
-        plan.stages = ws->cfg.pair_stages;
-        plan.band = ws->cfg.band;
-        plan.one_cta = !pair;
-        plan.wait_hint_ns = (uint32_t)ws->cfg.wait_hint_ns;
-        OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
-        OZA_CUDA_TRY(cudaEventRecord(o.g_done[c], st), "CUDA: event record");
-        OZA_CUDA_TRY(cudaStreamWaitEvent(o.s_crt, o.g_done[c], 0), "CUDA: stream wait");
-        OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->shiftA + r0,
-                                          ws->shiftB, C + r0 * N, ex->sms, o.s_crt),
-                     "step4 crt");
-    }
-    OZA_CUDA_TRY(cudaEventRecord(o.end, o.s_crt), "CUDA: event record");
-    OZA_CUDA_TRY(cudaStreamWaitEvent(st, o.end, 0), "CUDA: stream wait");
-    return OZA_OK;
-}
 
 cudaError_t host_pipe_init(oza_workspace* ws) {
     auto& h = ws->hp;
@@ -510,19 +406,6 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
     cudaStream_t st = ex->stream;
     const size_t M = ws->M, N = ws->N, K = ws->K;
 
-    if (!timings && K && ws->fused) {
-        // Overlapped stages: measured at 8192^3 / 4096^3 (S = 16) 8.7% / 2.8%
-        // faster than the sequential steps with 4 / 2 row chunks.
-        int chunks = ws->cfg.overlap_chunks;
-        if (chunks == 0) {
-            const int mt_all = (int)(ws->Mp / ((ws->pair && !ws->cfg.one_cta) ? oza::kTileMPair : oza::kTileM));
-            chunks = mt_all >= 32 ? 4 : (mt_all >= 4 ? 2 : 1);
-        }
-        if (chunks >= 2) {
-            OZA_CUDA_TRY(overlap_init(ws), "oza_gemm: overlap streams");
-            return gemm_overlapped(ws, A, B, C, chunks);
-        }
-    }
     if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[0], st), "CUDA: event record");
     if (K == 0) {
         // Empty inner dimension: the product is exactly zero.
@@ -594,14 +477,12 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg) {
     if (!ws) return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: null workspace");
     if (!cfg) {
-        ws->cfg = oza_gemm_config_t{0, 0, 0, 0, 0};
+        ws->cfg = oza_gemm_config_t{0, 0, 0, 0};
         return OZA_OK;
     }
     if (cfg->pair_stages != 0 && (cfg->pair_stages < 4 || cfg->pair_stages > 7))
         return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: pair_stages must be 0 or 4..7");
     if (cfg->band < 0 || cfg->band > 4096) return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: band out of range");
-    if (cfg->overlap_chunks < 0 || cfg->overlap_chunks > 16)
-        return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: overlap_chunks must be in [0, 16]");
     if (cfg->wait_hint_ns < 0 || cfg->wait_hint_ns > 1000000)
         return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: wait_hint_ns must be in [0, 1e6]");
     ws->cfg = *cfg;
@@ -622,8 +503,8 @@ oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, do
     const int bands[] = {8, 16, 32};
     if (ws->pair)
         for (int st = 4; st <= 7; ++st)
-            for (int b : bands) cand.push_back(oza_gemm_config_t{st, b, 0, saved.wait_hint_ns, saved.overlap_chunks});
-    for (int b : bands) cand.push_back(oza_gemm_config_t{0, b, 1, saved.wait_hint_ns, saved.overlap_chunks});
+            for (int b : bands) cand.push_back(oza_gemm_config_t{st, b, 0, saved.wait_hint_ns});
+    for (int b : bands) cand.push_back(oza_gemm_config_t{0, b, 1, saved.wait_hint_ns});
     float best_t = 1e30f;
     oza_gemm_config_t best_c = saved;
     for (const auto& c : cand) {
