@@ -456,6 +456,22 @@ __device__ __forceinline__ void slices16(const double (&vin)[16], int e, int bet
     }
 }
 
+// An all-zero chunk (tile padding, or zeros in the data) has zero residues
+// and zero Scheme I slices in every plane: store zero bytes and skip the
+// arithmetic.  -0.0 counts as zero; NaN does not.
+template <int E>
+__device__ __forceinline__ bool store_if_zero(const double (&v)[E], int planes, int8_t* dst, size_t plane) {
+    bool nz = false;
+#pragma unroll
+    for (int i = 0; i < E; ++i) nz = nz || (v[i] != 0.0);
+    if (nz) return false;
+    for (int s = 0; s < planes; ++s) {
+        if constexpr (E == 16) *reinterpret_cast<uint4*>(dst + (size_t)s * plane) = make_uint4(0, 0, 0, 0);
+        else *reinterpret_cast<uint2*>(dst + (size_t)s * plane) = make_uint2(0, 0);
+    }
+    return true;
+}
+
 // A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per E
 // consecutive columns of a row (E = 8 for Scheme II, 8-byte stores per plane;
 // 16 for Scheme I), coalesced.  Scheme II is instantiated per slice count SC
@@ -482,6 +498,7 @@ __device__ __forceinline__ void slice_rows_chunk(const double* __restrict__ A, l
         for (int i = 0; i < E; ++i) v[i] = 0.0;
     }
     int8_t* dst = out + (size_t)r * cols_p + c0;
+    if (store_if_zero<E>(v, SCHEME == 2 ? SC : S, dst, plane)) return;
     if (SCHEME == 2) {
         residuesE<SC, WIDE, E>(v, sh, pow2_or_zero(sh), dst, plane);
     } else {
@@ -531,6 +548,7 @@ __device__ __forceinline__ void slice_cols_tile(const double* __restrict__ B, lo
     for (int i = 0; i < 16; ++i) v[i] = tile[kg * 16 + i][lane];
     const size_t plane = (size_t)Np * (size_t)Kp;
     int8_t* dst = out + (size_t)n * Kp + k0 + kg * 16;
+    if (store_if_zero<16>(v, SCHEME == 2 ? SC : S, dst, plane)) return;
     if (SCHEME == 2) {
         residuesE<SC, WIDE, 16>(v, sh, pow2_or_zero(sh), dst, plane);
     } else {

@@ -185,3 +185,25 @@ def test_gemm_configurations_are_bit_identical(executor, scheme, S):
     assert ms > 0 and W.get_gemm_config() == cfg
     with pytest.raises(ValueError):
         W.set_gemm_config(9, 16, False)
+
+
+@pytest.mark.parametrize("scheme,S", [(2, 7), (2, 16), (2, 19), (1, 4)])
+def test_all_zero_chunks_bit_exact(executor, scheme, S):
+    """Chunks whose values are all zero (padding, zero rows, zeroed blocks,
+    -0.0) skip the residue arithmetic; every stage stays bit-identical."""
+    oz = _oz()
+    from oracle import Oracle
+    M, N, K = 300, 270, 400
+    A = oz.generate_matrix(M, K, 1.0, 61)
+    B = oz.generate_matrix(K, N, 1.0, 62)
+    A[5] = 0.0
+    A[:, 16:48] = 0.0
+    A[40:60, 200:216] = -0.0
+    A[7, 3] = -0.0
+    B[:, 9] = 0.0
+    B[128:256, 100:140] = 0.0
+    B[300:, :] = 0.0
+    got = run_pipeline(oz, executor, scheme, A, B, S)
+    ref = (Oracle.scheme2 if scheme == 2 else Oracle.scheme1)(A, B, S)
+    _check_all(got, ref)
+    _padding_zero(got)
