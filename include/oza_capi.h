@@ -144,6 +144,14 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
 
+/* Self-test of failure detection: one kernel waits, through the same bounded
+ * mbarrier wait as the GEMM kernels, on a barrier that nothing arrives on.
+ * The wait gives up after limit_s (0 < limit_s <= 5) and the kernel returns;
+ * *code receives the device error code (1: a wait expired), *elapsed_s
+ * (optional) the kernel's device time.  The context stays usable.
+ * Extension: the reference has no device-side wait. */
+oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code, double* elapsed_s);
+
 /* ---- GEMM tuning ------------------------------------------------------------ */
 /* Step-3 kernel configuration of a workspace (0 fields: library defaults).
  *   pair_stages  TMA pipeline depth of the CTA-pair kernel, 4..7 (default 6)

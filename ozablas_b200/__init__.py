@@ -26,7 +26,7 @@ __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
-    "autotune_slices", "GroupGemm", "Server", "slices_for_target", "ozaki_gemm_host",
+    "autotune_slices", "GroupGemm", "Server", "slices_for_target", "ozaki_gemm_host", "selftest_wait_timeout",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -129,6 +129,7 @@ def lib() -> ctypes.CDLL:
         "oza_ws_get_info": (I, [P, ctypes.POINTER(_WsInfo)]),
         "oza_gemm": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
         "oza_gemm_host": (I, [P, P, P, P, ctypes.POINTER(_Timings)]),
+        "oza_selftest_wait_timeout": (I, [P, ctypes.c_double, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]),
         "oza_ws_set_gemm_config": (I, [P, ctypes.POINTER(_GemmConfig)]),
         "oza_ws_get_gemm_config": (I, [P, ctypes.POINTER(_GemmConfig)]),
         "oza_autotune_gemm": (I, [P, P, P, P, ctypes.POINTER(_GemmConfig), ctypes.POINTER(ctypes.c_float)]),
@@ -531,6 +532,15 @@ def ozaki_gemm_host(ws, A, B, C, timings: OzaTimings | None = None) -> None:
     if timings is not None:
         for f, _ in _Timings._fields_:
             setattr(timings, f, float(getattr(t, f)))
+
+
+def selftest_wait_timeout(executor, limit_s: float = 0.2):
+    """Run one bounded device wait that nothing satisfies; returns (device
+    error code, kernel seconds).  Code 1 means the wait expired and reported."""
+    code = ctypes.c_int()
+    el = ctypes.c_double()
+    _check(lib().oza_selftest_wait_timeout(executor.handle, float(limit_s), ctypes.byref(code), ctypes.byref(el)))
+    return code.value, el.value
 
 
 def generate_matrix(rows: int, cols: int, phi: float = 0.5, seed: int = 42):

@@ -630,6 +630,35 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
     return OZA_OK;
 }
 
+oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code, double* elapsed_s) {
+    if (!ex || !code) return fail(OZA_INVALID_ARG, "oza_selftest_wait_timeout: null argument");
+    if (!(limit_s > 0.0) || limit_s > 5.0) return fail(OZA_INVALID_ARG, "oza_selftest_wait_timeout: limit in (0, 5] s");
+    DeviceGuard g(ex->device);
+    if (!g.ok) return fail(OZA_CUDA_ERROR, "CUDA: Failed to set device %d", ex->device);
+    int* buf = nullptr;
+    OZA_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&buf), 2 * sizeof(int)), "oza_selftest_wait_timeout: alloc");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMemset(buf, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, ex->stream);
+    if (e == cudaSuccess) e = oza::launch_wait_probe(buf, (unsigned long long)(limit_s * 1e9), buf + 1, ex->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, ex->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    int host[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(host, buf, sizeof(host), cudaMemcpyDeviceToHost);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(e, "oza_selftest_wait_timeout");
+    if (host[1]) return fail(OZA_CUDA_ERROR, "oza_selftest_wait_timeout: the wait returned without an arrival");
+    *code = host[0];
+    if (elapsed_s) *elapsed_s = ms * 1e-3;
+    return OZA_OK;
+}
+
 // ---------------------------------------------------------------- host utilities
 oza_status_t oza_generate_matrix(int rows, int cols, double phi, int seed, double* out) {
     if (rows < 0 || cols < 0 || (!out && rows && cols)) return fail(OZA_INVALID_ARG, "oza_generate_matrix: bad argument");

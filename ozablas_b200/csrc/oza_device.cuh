@@ -143,14 +143,14 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;
 // another role of the CTA already gave up (*abort != 0); on expiry it raises
 // *abort and records the error in the global error word.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* gerr,
-                                          uint32_t hint_ns = 0) {
+                                          uint32_t hint_ns = 0, uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     uint64_t t0 = globaltimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (hint_ns ? mbar_try_wait_hint(bar, parity, hint_ns) : mbar_try_wait(bar, parity)) return true;
         if (hint_ns || (it & 63u) == 0) {
             if (*abort) return false;
-            if (globaltimer_ns() - t0 > kWaitLimitNs) {
+            if (globaltimer_ns() - t0 > limit_ns) {
                 *abort = 1;
                 if (gerr) atomicExch(gerr, kErrWaitTimeout);
                 return false;

@@ -1471,6 +1471,24 @@ __global__ void __launch_bounds__(256) k_group_crt(const GroupProblemDev* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Self-test of the bounded waits: thread 0 waits, through the same mbar_wait
+// as the GEMM kernels, for a phase of an mbarrier that nothing arrives on.
+// The wait gives up after limit_ns, raises the abort flag and writes the
+// error code into *gerr; *status = 1 if the wait had (wrongly) succeeded.
+// ---------------------------------------------------------------------------
+__global__ void k_wait_probe(int* gerr, unsigned long long limit_ns, int* status) {
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        abort_flag = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *status = mbar_wait(&bar, 0, &abort_flag, gerr, 0, limit_ns) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 namespace {
@@ -2012,6 +2030,12 @@ cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t c
     if (ev) OZA_TRY(cudaEventRecord(ev[4], st));
 #undef OZA_TRY
     return cudaSuccess;
+}
+
+
+cudaError_t launch_wait_probe(int* gerr, unsigned long long limit_ns, int* status, cudaStream_t st) {
+    k_wait_probe<<<1, 32, 0, st>>>(gerr, limit_ns, status);
+    return cudaGetLastError();
 }
 
 }  // namespace oza

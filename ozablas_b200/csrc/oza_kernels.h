@@ -120,6 +120,10 @@ size_t group_plan_units(const GroupPlan* p);
 size_t group_plan_table_bytes(const GroupPlan* p);
 int group_plan_launches(const GroupPlan* p);   // kernel launches per call
 
+// One bounded wait on an mbarrier that nothing arrives on (self-test of the
+// wait bound): *gerr receives the device error code, *status 1 if it returned early.
+cudaError_t launch_wait_probe(int* gerr, unsigned long long limit_ns, int* status, cudaStream_t st);
+
 // Sets the text returned by oza_last_error_string() on this thread.
 void set_last_error(const char* msg);
 

@@ -164,3 +164,8 @@ def test_slices_for_target_is_a_monotone_lookup():
     assert f(1e-17, 1024, 0.5) == 21
     with pytest.raises(ValueError):
         f(0.0, 1024, 0.5)
+
+
+def test_selftest_rejects_null_executor():
+    code = ctypes.c_int()
+    assert oz.lib().oza_selftest_wait_timeout(None, 0.1, ctypes.byref(code), None) == oz.OZA_INVALID_ARG
