@@ -86,7 +86,8 @@ struct oza_workspace {
         double* dC = nullptr;
         cudaStream_t cin = nullptr, cout = nullptr;
         cudaEvent_t t0 = nullptr, t1 = nullptr, b_in = nullptr, out_done = nullptr;
-        cudaEvent_t a_in[8] = {}, done[8] = {};
+        static constexpr int kMaxChunks = 16;
+        cudaEvent_t a_in[kMaxChunks] = {}, done[kMaxChunks] = {};
     } hp;
 };
 
@@ -106,7 +107,7 @@ void ws_release(oza_workspace* ws) {
     cudaEvent_t evs[] = {h.t0, h.t1, h.b_in, h.out_done};
     for (cudaEvent_t e : evs)
         if (e) cudaEventDestroy(e);
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < oza_workspace::HostPipe::kMaxChunks; ++i) {
         if (h.a_in[i]) cudaEventDestroy(h.a_in[i]);
         if (h.done[i]) cudaEventDestroy(h.done[i]);
     }
@@ -126,7 +127,7 @@ cudaError_t host_pipe_init(oza_workspace* ws) {
     if (e == cudaSuccess) e = cudaEventCreate(&h.t1);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.b_in, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.out_done, cudaEventDisableTiming);
-    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+    for (int i = 0; i < oza_workspace::HostPipe::kMaxChunks && e == cudaSuccess; ++i) {
         e = cudaEventCreateWithFlags(&h.a_in[i], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.done[i], cudaEventDisableTiming);
     }
@@ -562,7 +563,9 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         const bool pair = ws->pair && !ws->cfg.one_cta;
         const size_t tile_m = pair ? oza::kTileMPair : oza::kTileM;
         const int mt_all = (int)(ws->Mp / tile_m);
-        const int R0 = mt_all < 8 ? mt_all : 8;
+        // 16 chunks: the exposed tail after the last A chunk lands (its
+        // GEMM, CRT and copy-out) is 1/16 of the compute and of C.
+        const int R0 = std::min(mt_all, (int)oza_workspace::HostPipe::kMaxChunks);
         const int q = (mt_all + R0 - 1) / R0;   // m-tiles per chunk
         const int R = (mt_all + q - 1) / q;
         OZA_CUDA_TRY(cudaStreamWaitEvent(h.cin, h.t0, 0), "CUDA: stream wait");
