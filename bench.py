@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--phi", type=float, default=0.5)
     p.add_argument("--cpu-sample", type=int, default=512, help="rows/cols of the CPU block sample")
     p.add_argument("--no-extras", action="store_true", help="skip DGEMM / reference-GPU / accuracy side numbers")
-    p.add_argument("--suite", default=None, choices=["precision", "grouped", "serve"],
+    p.add_argument("--suite", default=None, choices=["precision", "grouped", "serve", "sweep"],
                    help="precision: precision-targeted rectangular GEMMs with the slice count autotuned to "
                         "native DGEMM's error (one JSON line per shape and scheme); grouped: 512 independent "
                         "GEMMs as one grouped launch replayed from a CUDA graph vs 512 plain calls")
@@ -490,23 +490,29 @@ def reference_gpu_tflops(args, dA, dB, stream):
 PRECISION_SHAPES = [("tall_skinny", 16384, 16384, 1024), ("deep_k", 1024, 1024, 65536)]
 
 
+PRECISION_UP_ROWS, PRECISION_DOWN_ROWS = (1, 17), (5, 33)
+
+
 def precision_inputs(M, N, K, phi=4.0, zero_frac=0.05, seed=42):
-    """phi = 4 inputs with 5% exact zeros and a few rows of A and columns of B
-    (rows and columns of C) scaled by 2^+-300."""
+    """phi = 4 inputs (A seed 42, B seed 43) with 5% exact zeros (an independent
+    Bernoulli(0.05) mask over A then B from an MT19937 seeded 1234) and rows
+    {1, 17} of A and columns {1, 17} of B scaled by 2^300, rows and columns
+    {5, 33} by 2^-300 (rows and columns of C)."""
     import numpy as np
     import ozablas_b200 as oz
     A = oz.generate_matrix(M, K, phi, seed)
     B = oz.generate_matrix(K, N, phi, seed + 1)
-    rng = np.random.default_rng(seed)
-    A[rng.random(A.shape) < zero_frac] = 0.0
-    B[rng.random(B.shape) < zero_frac] = 0.0
-    ra = rng.choice(M, 6, replace=False)
-    cb = rng.choice(N, 6, replace=False)
-    A[ra[:3]] *= 2.0 ** 300
-    A[ra[3:]] *= 2.0 ** -300
-    B[:, cb[:3]] *= 2.0 ** 300
-    B[:, cb[3:]] *= 2.0 ** -300
-    return A, B, sorted(int(i) for i in ra), sorted(int(j) for j in cb)
+    mask = np.random.RandomState(1234)
+    A[mask.random_sample(A.shape) < zero_frac] = 0.0
+    B[mask.random_sample(B.shape) < zero_frac] = 0.0
+    for i in PRECISION_UP_ROWS:
+        A[i] *= 2.0 ** 300
+        B[:, i] *= 2.0 ** 300
+    for i in PRECISION_DOWN_ROWS:
+        A[i] *= 2.0 ** -300
+        B[:, i] *= 2.0 ** -300
+    idx = sorted(PRECISION_UP_ROWS + PRECISION_DOWN_ROWS)
+    return A, B, idx, idx
 
 
 def run_precision_suite(args, local):
@@ -566,7 +572,8 @@ def run_precision_suite(args, local):
                 "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                 "config": {"workload": f"precision_{name}_{M}x{N}x{K}", "M": M, "N": N, "K": K,
                            "scheme": scheme, "phi": 4.0, "zeros": 0.05,
-                           "scaled": "3 rows of A and 3 columns of B by 2^300, 3 each by 2^-300",
+                           "scaled": "rows {1,17} of A and columns {1,17} of B by 2^300, {5,33} by 2^-300",
+                           "zero_mask": "Bernoulli(0.05), MT19937 seed 1234",
                            "input_seed": 42},
                 "slices": S, "target_met_on_tuning_block": met,
                 "target_rel_err": target, "tuned_block_err": tuned,
@@ -583,6 +590,77 @@ def run_precision_suite(args, local):
             torch.cuda.empty_cache()
         del dA, dB, dD
         torch.cuda.empty_cache()
+
+
+# ------------------------------------------------------------------ slice-count sweep
+SWEEP_SIZES = (4096, 8192)
+SWEEP_PHIS = (0.5, 2.0, 4.0)
+SWEEP_SLICES = (4, 6, 8, 10, 12, 14, 16)
+
+
+def run_sweep_suite(args, local):
+    """Square Scheme I and Scheme II GEMMs, n in {4096, 8192}, phi in {0.5, 2, 4},
+    slices 4..16: per-step times (OzaTimings, median of 5 after 2 warm-ups),
+    step 1/2/4 GB/s of algorithmic bytes, step 3 INT8 TOPS against the INT8
+    peak, and the maximum relative error over a seeded 64 x 64 block of C
+    against the double-double GPU reference, beside cuBLAS DGEMM's."""
+    import torch
+    import ozablas_b200 as oz
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ex = oz.CudaExecutor(local)
+    stream = torch.cuda.current_stream(dev)
+    ex.set_stream(stream.cuda_stream)
+    peaks, peak_src = load_peaks()
+    int8_peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
+    for n in SWEEP_SIZES:
+        for phi in SWEEP_PHIS:
+            dA = torch.from_numpy(oz.generate_matrix(n, n, phi, 42)).to(dev)
+            dB = torch.from_numpy(oz.generate_matrix(n, n, phi, 43)).to(dev)
+            dC = torch.empty(n, n, dtype=torch.float64, device=dev)
+            for _ in range(2):
+                torch.matmul(dA, dB, out=dC)
+            dms = time_events(lambda: torch.matmul(dA, dB, out=dC), 5, stream)
+            derr = oz.block_error(ex, dA, dB, dC, n, n, n, 64, 7)
+            flops = 2.0 * n ** 3
+            for scheme in (2, 1):
+                for S in SWEEP_SLICES:
+                    W = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(ex, n, n, n, S)
+                    gemm = oz.ozaki_scheme2_gemm if scheme == 2 else oz.ozaki_scheme1_gemm
+                    t = oz.OzaTimings()
+                    for _ in range(2):
+                        gemm(W, dA, dB, dC, t)
+                    runs = []
+                    for _ in range(5):
+                        gemm(W, dA, dB, dC, t)
+                        runs.append((t.step1_ms, t.step2_ms, t.step3_ms, t.step4_ms, t.total_ms))
+                    med = [statistics.median(r[i] for r in runs) for i in range(5)]
+                    err = oz.block_error(ex, dA, dB, dC, n, n, n, 64, 7)
+                    G = S if scheme == 2 else S * (S + 1) // 2
+                    in_b = 8.0 * 2 * n * n
+                    b1 = in_b + 4.0 * 2 * n
+                    b2 = in_b + 4.0 * 2 * n + S * 2.0 * n * n
+                    b4 = (S if scheme == 2 else 4 * S) * 1.0 * n * n + 8.0 * n * n
+                    tops = 2.0 * n ** 3 * G / (med[2] * 1e-3) / 1e12
+                    print(json.dumps({
+                        "suite": "sweep", "metric": METRIC, "value": flops / (med[4] * 1e-3) / 1e12, "unit": UNIT,
+                        "higher_is_better": True,
+                        "config": {"workload": f"scheme{'II' if scheme == 2 else 'I'}_dgemm_{n}^3", "n": n,
+                                   "phi": phi, "scheme": scheme, "slices": S, "input_seeds": [42, 43]},
+                        "steps_ms": dict(zip(("step1_ms", "step2_ms", "step3_ms", "step4_ms", "total_ms"), med)),
+                        "step1_gbs": b1 / (med[0] * 1e-3) / 1e9, "step2_gbs": b2 / (med[1] * 1e-3) / 1e9,
+                        "step4_gbs": b4 / (med[3] * 1e-3) / 1e9,
+                        "step3_int8_tops": tops, "step3_frac_of_int8_peak": tops / int8_peak,
+                        "int8_peak": f"{int8_peak:.0f} TOPS = 2 x bf16 {peak_src}",
+                        "max_rel_err": err, "cublas_dgemm_max_rel_err": derr,
+                        "cublas_dgemm_tflops": flops / (dms * 1e-3) / 1e12,
+                        "error_reference": "double-double GPU GEMM on a 64 x 64 block (seed 7)",
+                    }), flush=True)
+                    del W
+                    torch.cuda.empty_cache()
+            del dA, dB, dC
+            torch.cuda.empty_cache()
 
 
 # ------------------------------------------------------------------ grouped suite
@@ -711,13 +789,20 @@ def run_grouped_suite(args, local):
 
 # ------------------------------------------------------------------ serving suite
 SERVE_BUDGET = 120 << 30
-SERVE_WS_CAP = 2 << 30
+SERVE_WS_CAP = 2e9
+
+
+def ref_workspace_bytes(M, N, K, S):
+    """The reference's Scheme II workspace size (workspace.cpp: shifts, slices
+    and INT32 products)."""
+    return 4 * (M + N) + S * (M * K + K * N) + 4 * S * M * N
 
 
 def serve_requests(n, seed=99):
-    """M, N, K log-uniform in [128, 8192] (K capped so the workspace is at most
-    2 GiB), phi in {0.5, 2}, target in {1e-12, 1e-15} -> slice count from the
-    calibrated table (20 where it is not reached)."""
+    """M, N, K log-uniform in [128, 8192] (K capped so the reference's workspace
+    formula 4(M+N) + S(MK+KN) + 4S MN is at most 2 GB), phi in {0.5, 2}, target
+    in {1e-12, 1e-15} -> slice count from the calibrated table (20 where it is
+    not reached)."""
     import numpy as np
     import ozablas_b200 as oz
     rng = np.random.default_rng(seed)
@@ -727,7 +812,7 @@ def serve_requests(n, seed=99):
         phi = float(rng.choice([0.5, 2.0]))
         target = float(rng.choice([1e-12, 1e-15]))
         S = oz.slices_for_target(target, K, phi)
-        while oz.Server.request_bytes(M, N, K, min(S, 20)) > SERVE_WS_CAP and K > 128:
+        while ref_workspace_bytes(M, N, K, min(S, 20)) > SERVE_WS_CAP and K > 128:
             K = max(128, K * 3 // 4)
             S = oz.slices_for_target(target, K, phi)
         out.append(dict(M=M, N=N, K=K, phi=phi, target=target, S=min(S, 20), table_reaches_target=S <= 20))
@@ -850,7 +935,7 @@ def run_serve_suite(args, local):
     base = {
         "suite": "serve", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
         "config": {"workload": f"served_dgemm_stream_{len(reqs)}_requests",
-                   "dims": "M, N, K log-uniform in [128, 8192], K capped so the workspace is <= 2 GiB",
+                   "dims": "M, N, K log-uniform in [128, 8192], K capped so 4(M+N)+S(MK+KN)+4S*MN <= 2 GB",
                    "phi": [0.5, 2.0], "targets": [1e-12, 1e-15],
                    "slices": "oza_slices_for_target (20 where the table does not reach the target)",
                    "budget_bytes": SERVE_BUDGET, "max_inflight": 2, "max_batch": 64,
@@ -890,6 +975,9 @@ def run_serve_suite(args, local):
 
 def main():
     args = parse()
+    if args.suite == "sweep":
+        run_sweep_suite(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     if args.suite == "serve":
         run_serve_suite(args, int(os.environ.get("LOCAL_RANK", 0)))
         return
