@@ -156,14 +156,19 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
 /* Step-3 kernel configuration of a workspace (0 fields: library defaults).
  *   pair_stages  TMA pipeline depth of the CTA-pair kernel, 4..7 (default 6)
  *   band         m-tiles per rasterisation band (default 16)
- *   one_cta      1: one-CTA 128 x 256 tiles instead of CTA-pair 256 x 256 tiles
+ *   cta_pair     1: the cluster-launched CTA-pair kernel (256 x 256 tiles on two
+ *                SMs) instead of the default one-CTA kernel (128 x 256 tiles).
+ *                Same results and, measured, the same speed within +-2%.  Do
+ *                not run it concurrently with other kernels (another stream,
+ *                another workspace): runs that overlapped it with other
+ *                kernels stalled intermittently.
  *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
 typedef struct {
     int pair_stages;
     int band;
-    int one_cta;
+    int cta_pair;
     int wait_hint_ns;
 } oza_gemm_config_t;
 

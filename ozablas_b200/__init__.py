@@ -62,7 +62,7 @@ class _WsInfo(ctypes.Structure):
 
 
 class _GemmConfig(ctypes.Structure):
-    _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("one_cta", ctypes.c_int),
+    _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("cta_pair", ctypes.c_int),
                 ("wait_hint_ns", ctypes.c_int)]
 
 
@@ -299,10 +299,10 @@ class _Workspace:
         _check(lib().oza_ws_device_error(self._h, ctypes.byref(c)))
         return c.value
 
-    def set_gemm_config(self, pair_stages: int = 0, band: int = 0, one_cta: bool = False,
+    def set_gemm_config(self, pair_stages: int = 0, band: int = 0, cta_pair: bool = False,
                         wait_hint_ns: int = 0) -> None:
         """Step-3 kernel configuration (0: defaults); results are unaffected."""
-        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(one_cta)), int(wait_hint_ns))
+        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(cta_pair)), int(wait_hint_ns))
         _check(lib().oza_ws_set_gemm_config(self._h, ctypes.byref(cfg)))
 
     def get_gemm_config(self) -> dict:

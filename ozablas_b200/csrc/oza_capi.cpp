@@ -437,12 +437,12 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
-        plan.pair = ws->pair;
+        plan.pair = ws->pair && ws->cfg.cta_pair != 0;
         plan.ctc = ws->ctc;
         plan.coef = ws->fused ? ws->coef : nullptr;
         plan.stages = ws->cfg.pair_stages;
         plan.band = ws->cfg.band;
-        plan.one_cta = ws->cfg.one_cta != 0;
+        plan.one_cta = false;
         plan.wait_hint_ns = (uint32_t)ws->cfg.wait_hint_ns;
         OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[3], st), "CUDA: event record");
@@ -502,10 +502,8 @@ oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, do
     const oza_gemm_config_t saved = ws->cfg;
     std::vector<oza_gemm_config_t> cand;
     const int bands[] = {8, 16, 32};
-    if (ws->pair)
-        for (int st = 4; st <= 7; ++st)
-            for (int b : bands) cand.push_back(oza_gemm_config_t{st, b, 0, saved.wait_hint_ns});
-    for (int b : bands) cand.push_back(oza_gemm_config_t{0, b, 1, saved.wait_hint_ns});
+    // One-CTA kernel only: the CTA-pair kernel stays an explicit opt-in.
+    for (int b : bands) cand.push_back(oza_gemm_config_t{0, b, 0, saved.wait_hint_ns});
     float best_t = 1e30f;
     oza_gemm_config_t best_c = saved;
     for (const auto& c : cand) {
@@ -560,9 +558,11 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         // only) and reconstructed, and its rows of C go back while the next
         // chunk is computed.  Copies in and out run on their own streams.
         const int offset = ws->k_param;
-        const bool pair = ws->pair && !ws->cfg.one_cta;
+        const bool pair = ws->pair && ws->cfg.cta_pair != 0;
         const size_t tile_m = pair ? oza::kTileMPair : oza::kTileM;
-        const int mt_all = (int)(ws->Mp / tile_m);
+        // Tiles that hold rows of A (Mp may be rounded further, to 256 rows,
+        // than the 128-row tiles of the one-CTA kernel need).
+        const int mt_all = (int)((M + tile_m - 1) / tile_m);
         // 16 chunks: the exposed tail after the last A chunk lands (its
         // GEMM, CRT and copy-out) is 1/16 of the compute and of C.
         const int R0 = std::min(mt_all, (int)oza_workspace::HostPipe::kMaxChunks);
@@ -579,8 +579,8 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
                      "step2 cols");
         for (int c = 0; c < R; ++c) {
             const size_t r0 = (size_t)c * q * tile_m;
-            const size_t rows_p = std::min((size_t)q * tile_m, ws->Mp - r0);
-            const size_t rows = std::min(M, r0 + rows_p) - r0;   // >= 1: chunks start on tile boundaries below Mp
+            const size_t rows_p = std::min((size_t)q * tile_m, (size_t)mt_all * tile_m - r0);
+            const size_t rows = std::min(M, r0 + rows_p) - r0;   // >= 1: every chunk starts below M
             OZA_CUDA_TRY(cudaMemcpyAsync(h.dA + r0 * K, hA + r0 * K, rows * K * sizeof(double),
                                          cudaMemcpyHostToDevice, h.cin),
                          "H2D A chunk");

@@ -168,7 +168,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     plan.pairs = oza::make_pairs(scheme, slices);
     plan.err = err;
     plan.sms = sms;
-    plan.pair = pair;
+    plan.pair = false;
     plan.ctc = scheme == OZA_SCHEME1 ? reinterpret_cast<int32_t*>(out) : nullptr;
     plan.coef = scheme == OZA_SCHEME2 ? out : nullptr;
     NA_TRY(oza::launch_gemm_i8(plan, st), "step 3");

@@ -5,7 +5,8 @@
 //  * one scheduler thread admits queued requests in arrival order while their
 //    workspaces fit in a device arena of the configured budget and a stream
 //    slot is free, and launches everything it admitted as one grouped batch
-//    (the grouped kernels of oza_kernels.cu) on that slot's stream;
+//    (the grouped kernels of oza_kernels.cu) on that slot's stream -- a batch
+//    of one request runs the single-GEMM launch sequence instead;
 //  * up to max_inflight batches run at once on separate streams, so requests
 //    that arrive while a batch is on the GPU are admitted as soon as a slot and
 //    memory free up, and their work overlaps on the device;
@@ -193,7 +194,8 @@ bool oza_server::poll() {
             (q != cudaSuccess || sl.launch_failed) ? OZA_CUDA_ERROR : (code ? OZA_TIMEOUT : OZA_OK);
         for (Request* r : sl.reqs) arena.release(r->ws_off, r->ws_bytes);
         arena.release(sl.blk_off, sl.blk_bytes);
-        arena.release(sl.tab_off, sl.tab_bytes);
+        if (sl.tab_bytes) arena.release(sl.tab_off, sl.tab_bytes);
+        sl.tab_bytes = 0;
         oza::group_plan_destroy(sl.plan);
         sl.plan = nullptr;
         sl.busy = false;
@@ -280,22 +282,30 @@ bool oza_server::launch() {
         p.colmax = colmax + cofs;
         cofs += r->N;
     }
+    // A batch of one runs the single-GEMM launch sequence (no device tables);
+    // larger batches run the grouped kernels.
+    const bool single = batch.size() == 1;
     oza::GroupPlan* plan = nullptr;
-    cudaError_t e = oza::group_plan_build(probs.data(), (int)probs.size(), err, &plan);
-    if (e != cudaSuccess) {
-        arena.release(sl->blk_off, sl->blk_bytes);
-        requeue("plan");
-        std::lock_guard<std::mutex> lk(mu);
-        failed = true;
-        fail_msg = std::string("batch plan: ") + cudaGetErrorString(e);
-        return false;
-    }
-    sl->tab_bytes = oza::group_plan_table_bytes(plan);
-    if (!arena.alloc(sl->tab_bytes, &sl->tab_off)) {
-        oza::group_plan_destroy(plan);
-        arena.release(sl->blk_off, sl->blk_bytes);
-        requeue("no memory for the batch tables");
-        return false;
+    cudaError_t e = cudaSuccess;
+    sl->tab_bytes = 0;
+    if (!single) {
+        e = oza::group_plan_build(probs.data(), (int)probs.size(), err, &plan);
+        if (e != cudaSuccess) {
+            arena.release(sl->blk_off, sl->blk_bytes);
+            requeue("plan");
+            std::lock_guard<std::mutex> lk(mu);
+            failed = true;
+            fail_msg = std::string("batch plan: ") + cudaGetErrorString(e);
+            return false;
+        }
+        sl->tab_bytes = oza::group_plan_table_bytes(plan);
+        if (!arena.alloc(sl->tab_bytes, &sl->tab_off)) {
+            oza::group_plan_destroy(plan);
+            arena.release(sl->blk_off, sl->blk_bytes);
+            sl->tab_bytes = 0;
+            requeue("no memory for the batch tables");
+            return false;
+        }
     }
     const size_t need = kAlign + sl->tab_bytes;
     if (sl->pinned_cap < need) {
@@ -306,7 +316,8 @@ bool oza_server::launch() {
         if (cudaHostAlloc(reinterpret_cast<void**>(&sl->pinned), cap, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             oza::group_plan_destroy(plan);
-            arena.release(sl->tab_off, sl->tab_bytes);
+            if (sl->tab_bytes) arena.release(sl->tab_off, sl->tab_bytes);
+            sl->tab_bytes = 0;
             arena.release(sl->blk_off, sl->blk_bytes);
             requeue("pinned staging");
             std::lock_guard<std::mutex> lk(mu);
@@ -316,13 +327,42 @@ bool oza_server::launch() {
         }
         sl->pinned_cap = cap;
     }
-    std::memcpy(sl->pinned + kAlign, oza::group_plan_image(plan), sl->tab_bytes);
-    void* tab = arena_base + sl->tab_off;
-    oza::group_plan_bind(plan, tab);
     const double t = now();
-    e = cudaMemcpyAsync(tab, sl->pinned + kAlign, sl->tab_bytes, cudaMemcpyHostToDevice, sl->st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), sl->st);
-    if (e == cudaSuccess) e = oza::group_plan_launch(plan, colmax, ncol, ex->sms, sl->st, nullptr);
+    if (single) {
+        const oza::GroupProblem& p = probs[0];
+        oza::GemmPlan g;
+        g.a_planes = p.a_planes;
+        g.b_planes = p.b_planes;
+        g.planes = p.S;
+        g.Mp = p.Mp;
+        g.Np = p.Np;
+        g.Kp = p.Kp;
+        g.pairs = oza::make_pairs(OZA_SCHEME2, p.S);
+        g.err = err;
+        g.sms = ex->sms;
+        g.pair = false;   // one-CTA kernel: batches on other slots run concurrently
+        g.ctc = nullptr;
+        g.coef = p.coef;
+        e = cudaMemsetAsync(err, 0, sizeof(int), sl->st);
+        if (e == cudaSuccess) e = oza::launch_stats_rows(p.A, p.M, p.K, p.k_param, p.shiftA, ex->sms, sl->st);
+        if (e == cudaSuccess) e = oza::launch_stats_cols(p.B, p.K, p.N, p.colmax, ex->sms, sl->st);
+        if (e == cudaSuccess)
+            e = oza::launch_slice_rows(OZA_SCHEME2, p.A, p.M, p.K, p.shiftA, p.S, 0, p.k_param, p.a_planes, p.Mp, p.Kp,
+                                       ex->sms, sl->st);
+        if (e == cudaSuccess)
+            e = oza::launch_slice_cols(OZA_SCHEME2, p.B, p.K, p.N, p.colmax, p.k_param, p.S, 0, p.shiftB, p.b_planes,
+                                       p.Np, p.Kp, sl->st);
+        if (e == cudaSuccess) e = oza::launch_gemm_i8(g, sl->st);
+        if (e == cudaSuccess)
+            e = oza::launch_crt_coef(p.coef, p.Mp, p.Np, p.M, p.N, p.S, p.shiftA, p.shiftB, p.C, ex->sms, sl->st);
+    } else {
+        std::memcpy(sl->pinned + kAlign, oza::group_plan_image(plan), sl->tab_bytes);
+        void* tab = arena_base + sl->tab_off;
+        oza::group_plan_bind(plan, tab);
+        e = cudaMemcpyAsync(tab, sl->pinned + kAlign, sl->tab_bytes, cudaMemcpyHostToDevice, sl->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), sl->st);
+        if (e == cudaSuccess) e = oza::group_plan_launch(plan, colmax, ncol, ex->sms, sl->st, nullptr);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(sl->pinned, err, sizeof(int), cudaMemcpyDeviceToHost, sl->st);
     if (e == cudaSuccess) e = cudaEventRecord(sl->done, sl->st);
     // Wake the scheduler as soon as the batch is done (after the event, so the
