@@ -163,6 +163,12 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
  *                another workspace): runs that overlapped it with other
  *                kernels stalled intermittently.
  *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
+ *   overlap_chunks  Scheme II fused path, calls without timings, one-CTA
+ *                kernel: >= 2 splits the GEMM into that many row chunks and
+ *                overlaps A's slicing and each chunk's reconstruction with
+ *                the GEMM on two more streams; 1: the steps in order; 0: 4
+ *                chunks from 48 row tiles of 128, 2 from 8, else 1.  Calls
+ *                with timings, and the CTA-pair kernel, run the steps in order.
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
 typedef struct {
@@ -170,6 +176,7 @@ typedef struct {
     int band;
     int cta_pair;
     int wait_hint_ns;
+    int overlap_chunks;
 } oza_gemm_config_t;
 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg); /* NULL: defaults */

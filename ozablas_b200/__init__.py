@@ -63,7 +63,7 @@ class _WsInfo(ctypes.Structure):
 
 class _GemmConfig(ctypes.Structure):
     _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("cta_pair", ctypes.c_int),
-                ("wait_hint_ns", ctypes.c_int)]
+                ("wait_hint_ns", ctypes.c_int), ("overlap_chunks", ctypes.c_int)]
 
 
 class _GroupInfo(ctypes.Structure):
@@ -300,9 +300,9 @@ class _Workspace:
         return c.value
 
     def set_gemm_config(self, pair_stages: int = 0, band: int = 0, cta_pair: bool = False,
-                        wait_hint_ns: int = 0) -> None:
+                        wait_hint_ns: int = 0, overlap_chunks: int = 0) -> None:
         """Step-3 kernel configuration (0: defaults); results are unaffected."""
-        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(cta_pair)), int(wait_hint_ns))
+        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(cta_pair)), int(wait_hint_ns), int(overlap_chunks))
         _check(lib().oza_ws_set_gemm_config(self._h, ctypes.byref(cfg)))
 
     def get_gemm_config(self) -> dict:

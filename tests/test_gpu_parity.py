@@ -181,6 +181,13 @@ def test_gemm_configurations_are_bit_identical(executor, scheme, S):
             C = torch.empty_like(ref)
             gemm(W, A, B, C)
             assert torch.equal(C.view(torch.int64), ref.view(torch.int64)), (stages, band, pair)
+    if scheme == 2:
+        for chunks in (1, 2, 3, 16):   # steps in order and overlapped stages: same bits
+            W.set_gemm_config(overlap_chunks=chunks)
+            for _ in range(3):
+                C = torch.full_like(ref, float("nan"))
+                gemm(W, A, B, C)
+                assert torch.equal(C.view(torch.int64), ref.view(torch.int64)), chunks
     W.set_gemm_config()
     cfg, ms = W.autotune_gemm(A, B, torch.empty_like(ref))
     assert ms > 0 and W.get_gemm_config() == cfg
