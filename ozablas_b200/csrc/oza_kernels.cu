@@ -1381,6 +1381,12 @@ __global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict_
 // launch works on problem ids[q] for start[q] <= b < start[q + 1], at local
 // tile b - start[q]; the bodies are the single-GEMM kernels' own.
 // ---------------------------------------------------------------------------
+// Work per block of the grouped slicers: 4 chunks per thread (rows) and 2
+// k-tiles per block (columns), so the block-to-problem search and the
+// problem loads are amortised and loads of one chunk overlap the next.
+constexpr int kGroupRowChunks = 4;
+constexpr int kGroupColTiles = 2;
+
 struct GroupProblemDev {
     const double* A;
     const double* B;
@@ -1440,10 +1446,15 @@ __global__ void __launch_bounds__(256, 3) k_group_slice_rows(const GroupProblemD
                                                              const __grid_constant__ GroupLaunchDev L) {
     const int q = group_find(L, blockIdx.x);
     const GroupProblemDev& P = probs[L.ids[q]];
-    const long long id = (blockIdx.x - L.start[q]) * 256 + threadIdx.x;
-    if (id >= P.Mp * (P.Kp / 8)) return;
-    slice_rows_chunk<2, SC, WIDE>(P.A, P.M, P.K, P.shiftA, SC, 0, P.a_planes, P.Kp, (size_t)P.Mp * (size_t)P.Kp,
-                                  id);
+    const long long total = P.Mp * (P.Kp / 8);
+    const long long base = (blockIdx.x - L.start[q]) * (256 * kGroupRowChunks) + threadIdx.x;
+#pragma unroll 1
+    for (int r = 0; r < kGroupRowChunks; ++r) {
+        const long long id = base + r * 256;
+        if (id >= total) return;
+        slice_rows_chunk<2, SC, WIDE>(P.A, P.M, P.K, P.shiftA, SC, 0, P.a_planes, P.Kp,
+                                      (size_t)P.Mp * (size_t)P.Kp, id);
+    }
 }
 
 // Tile (bx, by) of (Np/32) x (Kp/128) per problem.
@@ -1453,9 +1464,15 @@ __global__ void __launch_bounds__(256, 3) k_group_slice_cols(const GroupProblemD
     const int q = group_find(L, blockIdx.x);
     const GroupProblemDev& P = probs[L.ids[q]];
     const long long t = blockIdx.x - L.start[q];
-    const long long nx = P.Np / 32;
-    slice_cols_tile<2, SC, WIDE>(P.B, P.K, P.N, P.colmax, P.k_param, SC, 0, P.shiftB, P.b_planes, P.Np, P.Kp, t % nx,
-                                 t / nx);
+    const long long nx = P.Np / 32, ny = P.Kp / 128;
+#pragma unroll 1
+    for (int r = 0; r < kGroupColTiles; ++r) {
+        const long long by = (t / nx) * kGroupColTiles + r;
+        if (by >= ny) return;   // block-uniform
+        if (r) __syncthreads();  // the shared tile is reloaded
+        slice_cols_tile<2, SC, WIDE>(P.B, P.K, P.N, P.colmax, P.k_param, SC, 0, P.shiftB, P.b_planes, P.Np, P.Kp,
+                                     t % nx, by);
+    }
 }
 
 // 256 chunks of 4 columns per block over M x N.
@@ -1857,8 +1874,8 @@ cudaError_t group_plan_build(const GroupProblem* in, int count, int* err, GroupP
         switch (stage) {
             case 0: return (d.M + 7) / 8;
             case 1: return ((d.N + 63) / 64) * ((d.K + 255) / 256);
-            case 2: return (d.Mp * (d.Kp / 8) + 255) / 256;
-            case 3: return (d.Np / 32) * (d.Kp / 128);
+            case 2: return (d.Mp * (d.Kp / 8) + 256 * kGroupRowChunks - 1) / (256 * kGroupRowChunks);
+            case 3: return (d.Np / 32) * ((d.Kp / 128 + kGroupColTiles - 1) / kGroupColTiles);
             default: return (d.M * ((d.N + 3) / 4) + 255) / 256;
         }
     };
