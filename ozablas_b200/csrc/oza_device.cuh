@@ -316,13 +316,15 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, ui
 }
 
 // Arrive once on the barrier at this shared offset in both CTAs of the pair
-// when the pair's tcgen05.mma issued so far are complete.
+// when the pair's tcgen05.mma issued so far are complete: one commit per CTA,
+// each to a shared::cluster barrier address (mapa) of that CTA.
 __device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
-    asm volatile(
-        "{\n\t.reg .b16 m;\n\tmov.b16 m, 3;\n\t"
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m;\n\t}" ::"r"(
-            smem_u32(bar))
-        : "memory");
+    const uint32_t a = smem_u32(bar);
+    uint32_t r0, r1;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, 0;" : "=r"(r0) : "r"(a));
+    asm volatile("mapa.shared::cluster.u32 %0, %1, 1;" : "=r"(r1) : "r"(a));
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(r0) : "memory");
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(r1) : "memory");
 }
 
 }  // namespace oza

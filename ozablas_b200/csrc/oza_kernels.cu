@@ -1084,7 +1084,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_
 // 128 x 256 tile.  The even CTA issues the MMAs; TMA completions of both CTAs
 // are counted on its full barriers; MMA commits arrive on both CTAs'
 // barriers; both CTAs' epilogue warps release the accumulator on the even
-// CTA's acc_empty barrier.  No TMA multicast is used.
+// CTA's acc_empty barrier.  Every TMA load is a plain load into this CTA.
 constexpr int kPairTileM = 256;                   // rows of C per CTA pair
 constexpr int kPairABytes = 128 * kTileK;         // this CTA's 128 rows of A
 constexpr int kPairBBytes = 128 * kTileK;         // this CTA's half of B^T
