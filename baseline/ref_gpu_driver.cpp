@@ -1,6 +1,6 @@
 // ref_gpu_driver.cpp -- extern "C" handle over the reference's GPU pipeline.
 //
-// BASELINE INFRASTRUCTURE.  Linked by baseline/Makefile together with
+// Comparison infrastructure, not the product.  Linked by baseline/Makefile with
 // the reference's own sources (src/cuda/pipeline.cu, src/core/*.cpp,
 // src/ozablas.cpp) into baseline/_ref/libozablas_ref_gpu.so.  It drives the
 // unmodified reference through its public C++ API
