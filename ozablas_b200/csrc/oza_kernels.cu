@@ -919,78 +919,80 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
     const int total_units = src.count();
 
     if (warp == 0) {
-        // ---------------- TMA producer ----------------
-        int stage = 0;
-        uint32_t phase = 0;
-        long long issued = 0;
-        bool ok = true;
-        const CUtensorMap* last_map = nullptr;
-        for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
-            GemmUnit x;
-            src.get(u, x);
-            if (lane == 0 && x.tmA != last_map) {
-                tma_prefetch_desc(x.tmA);
-                tma_prefetch_desc(x.tmB);
-                last_map = x.tmA;
-            }
-            for (int p = x.p0; p < x.p1 && ok; ++p) {
-                const int arow = (int)(src.a_plane(p) * x.Mp + (long long)x.mt * kTileM);
-                const int brow = (int)(src.b_plane(p) * x.Np + (long long)x.nt * kTileN);
-                for (int kb = 0; kb < x.k_blocks; ++kb) {
-                    int w = 1;
-                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, err, hint);
-                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                    if (!ok) break;
-                    if (lane == 0) {
+        // ---------------- TMA producer (one lane) ----------------
+        // The whole role runs in lane 0: no per-k-block reconvergence of the
+        // warp, which would stall the issue stream between stages.
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            long long issued = 0;
+            bool ok = true;
+            const CUtensorMap* last_map = nullptr;
+            for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
+                GemmUnit x;
+                src.get(u, x);
+                if (x.tmA != last_map) {
+                    tma_prefetch_desc(x.tmA);
+                    tma_prefetch_desc(x.tmB);
+                    last_map = x.tmA;
+                }
+                for (int p = x.p0; p < x.p1 && ok; ++p) {
+                    const int arow = (int)(src.a_plane(p) * x.Mp + (long long)x.mt * kTileM);
+                    const int brow = (int)(src.b_plane(p) * x.Np + (long long)x.nt * kTileN);
+                    for (int kb = 0; kb < x.k_blocks; ++kb) {
+                        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, err, hint)) {
+                            ok = false;
+                            break;
+                        }
                         mbar_arrive_expect_tx(&full[stage], kABytes + kBBytes);
                         tma_load_2d(sA + stage * kABytes, x.tmA, &full[stage], kb * kTileK, arow);
                         tma_load_2d(sB + stage * kBBytes, x.tmB, &full[stage], kb * kTileK, brow);
-                    }
-                    __syncwarp();
-                    ++issued;
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
+                        ++issued;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
             }
-        }
-        if (!ok && lane == 0) {
-            // Let the copies already issued land before the CTA leaves.
-            long long n = issued < kStages ? issued : kStages;
-            volatile int no_abort = 0;
-            for (long long j = 0; j < n; ++j) {
-                long long idx = issued - 1 - j;
-                mbar_wait(&full[idx % kStages], (uint32_t)((idx / kStages) & 1), &no_abort, nullptr);
+            if (!ok) {
+                // Let the copies already issued land before the CTA leaves.
+                long long n = issued < kStages ? issued : kStages;
+                volatile int no_abort = 0;
+                for (long long j = 0; j < n; ++j) {
+                    long long idx = issued - 1 - j;
+                    mbar_wait(&full[idx % kStages], (uint32_t)((idx / kStages) & 1), &no_abort, nullptr);
+                }
             }
         }
+        __syncwarp();
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        constexpr uint32_t idesc = umma_idesc_i8(kTileM, kTileN);
-        int stage = 0;
-        uint32_t phase = 0;
-        int local = 0;
-        bool ok = true;
-        for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
-            GemmUnit x;
-            src.get(u, x);
-            const int acc = local & 1;
-            const uint32_t acc_phase = (local >> 1) & 1;
-            int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, err, hint);
-            ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-            if (!ok) break;
-            tc_fence_after();
-            const uint32_t d = tmem_base + acc * kAccCols;
-            uint32_t accumulate = 0;
-            for (int p = x.p0; p < x.p1 && ok; ++p) {
-                for (int kb = 0; kb < x.k_blocks; ++kb) {
-                    w = 1;
-                    if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, err, hint);
-                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                    if (!ok) break;
-                    tc_fence_after();
-                    if (lane == 0) {
+        // ---------------- MMA issuer (one lane) ----------------
+        if (lane == 0) {
+            constexpr uint32_t idesc = umma_idesc_i8(kTileM, kTileN);
+            int stage = 0;
+            uint32_t phase = 0;
+            int local = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++local) {
+                GemmUnit x;
+                src.get(u, x);
+                const int acc = local & 1;
+                const uint32_t acc_phase = (local >> 1) & 1;
+                if (!mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, err, hint)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + acc * kAccCols;
+                uint32_t accumulate = 0;
+                for (int p = x.p0; p < x.p1 && ok; ++p) {
+                    for (int kb = 0; kb < x.k_blocks; ++kb) {
+                        if (!mbar_wait(&full[stage], phase, abort_flag, err, hint)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
                         const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kABytes));
                         const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kBBytes));
 #pragma unroll
@@ -1000,25 +1002,23 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
                             accumulate = 1;
                         }
                         umma_commit(&empty[stage]);
-                    }
-                    __syncwarp();
-                    accumulate = 1;
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
+                if (!ok) break;
+                umma_commit(&acc_full[acc]);
             }
-            if (!ok) break;
-            if (lane == 0) umma_commit(&acc_full[acc]);
-            __syncwarp();
+            if (!ok) {
+                // Wait for the MMAs already issued before TMEM is released.
+                umma_commit(drain);
+                volatile int no_abort = 0;
+                mbar_wait(drain, 0, &no_abort, nullptr);
+            }
         }
-        if (!ok && lane == 0) {
-            // Wait for the MMAs already issued before TMEM is released.
-            umma_commit(drain);
-            volatile int no_abort = 0;
-            mbar_wait(drain, 0, &no_abort, nullptr);
-        }
+        __syncwarp();
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3;                 // TMEM lane quadrant this warp may access
