@@ -1141,48 +1141,48 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     const int total_units = G * args.total_tiles;
 
     if (warp == 0) {
-        // ---------------- TMA producer (both CTAs) ----------------
-        int stage = 0;
-        uint32_t phase = 0;
-        bool ok = true;
-        for (int u = pair_id; u < total_units && ok; u += num_pairs) {
-            const int grp = u / args.total_tiles;
-            int mt, nt;
-            tile_coords(u - grp * args.total_tiles, args, mt, nt);
-            for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kPairTileM + rank * 128);
-                const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN + rank * 128);
-                for (int kb = 0; kb < args.k_blocks; ++kb) {
-                    int w = 1;
-                    if (lane == 0) w = mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err, hint);
-                    ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                    if (!ok) break;
-                    if (lane == 0) {
+        // ---------------- TMA producer (both CTAs, one lane) ----------------
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int u = pair_id; u < total_units && ok; u += num_pairs) {
+                const int grp = u / args.total_tiles;
+                int mt, nt;
+                tile_coords(u - grp * args.total_tiles, args, mt, nt);
+                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
+                    const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kPairTileM + rank * 128);
+                    const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN + rank * 128);
+                    for (int kb = 0; kb < args.k_blocks; ++kb) {
+                        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err, hint)) {
+                            ok = false;
+                            break;
+                        }
                         const uint32_t fbar = mapa_shared(smem_u32(&full[stage]), 0);
                         if (leader) mbar_arrive_expect_tx(&full[stage], 2 * (kPairABytes + kPairBBytes));
                         tma_load_2d_pair(sA + stage * kPairABytes, &tmA, fbar, kb * kTileK, arow);
                         tma_load_2d_pair(sB + stage * kPairBBytes, &tmB, fbar, kb * kTileK, brow);
-                    }
-                    __syncwarp();
-                    if (++stage == kPairStages) {
-                        stage = 0;
-                        phase ^= 1;
+                        if (++stage == kPairStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
             }
-        }
-        if (!ok && leader && lane == 0) {
-            // Let the copies of both CTAs land (the leader's full barriers count them).
-            volatile int no_abort = 0;
-            for (int j = 0; j < kPairStages; ++j) {
-                int st = (stage + kPairStages - 1 - j) % kPairStages;
-                uint32_t ph = (st < stage) ? phase : (phase ^ 1);
-                mbar_wait(&full[st], ph, &no_abort, nullptr);
+            if (!ok && leader) {
+                // Let the copies of both CTAs land (the leader's full barriers count them).
+                volatile int no_abort = 0;
+                for (int j = 0; j < kPairStages; ++j) {
+                    int st = (stage + kPairStages - 1 - j) % kPairStages;
+                    uint32_t ph = (st < stage) ? phase : (phase ^ 1);
+                    mbar_wait(&full[st], ph, &no_abort, nullptr);
+                }
             }
         }
+        __syncwarp();
     } else if (warp == 1) {
-        // ---------------- MMA issuer (even CTA) ----------------
-        if (leader) {
+        // ---------------- MMA issuer (even CTA, one lane) ----------------
+        if (leader && lane == 0) {
             constexpr uint32_t idesc = umma_idesc_i8(kPairTileM, kTileN);
             int stage = 0;
             uint32_t phase = 0;
@@ -1192,32 +1192,28 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
                 const int grp = u / args.total_tiles;
                 const int acc = local & 1;
                 const uint32_t acc_phase = (local >> 1) & 1;
-                int w = 1;
-                if (lane == 0) w = mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err, hint);
-                ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                if (!ok) break;
+                if (!mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err, hint)) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t d = tmem_base + acc * kAccCols;
                 uint32_t accumulate = 0;
                 for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
                     for (int kb = 0; kb < args.k_blocks; ++kb) {
-                        w = 1;
-                        if (lane == 0) w = mbar_wait(&full[stage], phase, abort_flag, args.err, hint);
-                        ok = __shfl_sync(0xFFFFFFFFu, w, 0) != 0;
-                        if (!ok) break;
-                        tc_fence_after();
-                        if (lane == 0) {
-                            const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kPairABytes));
-                            const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kPairBBytes));
-#pragma unroll
-                            for (int k = 0; k < kTileK / 32; ++k) {
-                                umma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
-                                accumulate = 1;
-                            }
-                            umma_commit_pair(&empty[stage]);
+                        if (!mbar_wait(&full[stage], phase, abort_flag, args.err, hint)) {
+                            ok = false;
+                            break;
                         }
-                        __syncwarp();
-                        accumulate = 1;
+                        tc_fence_after();
+                        const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kPairABytes));
+                        const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kPairBBytes));
+#pragma unroll
+                        for (int k = 0; k < kTileK / 32; ++k) {
+                            umma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
+                            accumulate = 1;
+                        }
+                        umma_commit_pair(&empty[stage]);
                         if (++stage == kPairStages) {
                             stage = 0;
                             phase ^= 1;
@@ -1225,15 +1221,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
                     }
                 }
                 if (!ok) break;
-                if (lane == 0) umma_commit_pair(&acc_full[acc]);
-                __syncwarp();
+                umma_commit_pair(&acc_full[acc]);
             }
-            if (!ok && lane == 0) {
+            if (!ok) {
                 umma_commit_pair(drain);
                 volatile int no_abort = 0;
                 mbar_wait(drain, 0, &no_abort, nullptr);
             }
         }
+        __syncwarp();
     } else {
         // ---------------- epilogue (both CTAs, own TMEM) ----------------
         const int q = warp & 3;
