@@ -86,7 +86,7 @@ struct oza_workspace {
         double* dC = nullptr;
         cudaStream_t cin = nullptr, cout = nullptr;
         cudaEvent_t t0 = nullptr, t1 = nullptr, b_in = nullptr, out_done = nullptr;
-        static constexpr int kMaxChunks = 16;
+        static constexpr int kMaxChunks = 32;
         cudaEvent_t a_in[kMaxChunks] = {}, done[kMaxChunks] = {};
     } hp;
     // Overlapped device path: slicer and reconstruction streams, chunk events.
@@ -686,8 +686,11 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         // Tiles that hold rows of A (Mp may be rounded further, to 256 rows,
         // than the 128-row tiles of the one-CTA kernel need).
         const int mt_all = (int)((M + tile_m - 1) / tile_m);
-        // 16 chunks: the exposed tail after the last A chunk lands (its
-        // GEMM, CRT and copy-out) is 1/16 of the compute and of C.
+        // 32 chunks: the exposed tail after the last A chunk lands (its
+        // GEMM, CRT and copy-out) is 1/32 of the compute and of C.  At
+        // 8192^3 a chunk's compute (~0.28 ms) still keeps pace with its copy
+        // (~0.31 ms), and the call ends ~1 ms above the PCIe floor (1 GiB in
+        // with the copy-out of C running beside the second half).
         const int R0 = std::min(mt_all, (int)oza_workspace::HostPipe::kMaxChunks);
         const int q = (mt_all + R0 - 1) / R0;   // m-tiles per chunk
         const int R = (mt_all + q - 1) / q;

@@ -65,11 +65,13 @@ def test_host_gemm_rejects_device_and_misshaped_buffers(executor):
         oz.ozaki_gemm_host(ws, np.zeros((8, 7)), np.zeros((7, 8)), np.zeros((8, 8)))
 
 
-@pytest.mark.parametrize("M,N,K,S", [(257, 255, 129, 19), (2304, 512, 300, 12), (700, 130, 96, 8)])
+@pytest.mark.parametrize("M,N,K,S", [(257, 255, 129, 19), (2304, 512, 300, 12), (700, 130, 96, 8),
+                                     (4500, 136, 96, 8), (8300, 72, 40, 5)])
 @pytest.mark.parametrize("cta_pair", [False, True])
 def test_host_gemm_both_kernels(executor, M, N, K, S, cta_pair):
     """Row chunks of 128 (one-CTA kernel) and 256 rows (CTA-pair kernel) both
-    cover M exactly, also when M is not a multiple of the tile."""
+    cover M exactly, also when M is not a multiple of the tile and when a
+    chunk holds several tiles (more tiles than the 32 chunks)."""
     import torch
     A = oz.generate_matrix(M, K, 0.5, 13)
     B = oz.generate_matrix(K, N, 0.5, 14)
