@@ -62,6 +62,9 @@ def parse():
                    help="offered loads as fractions of the batched server's measured capacity")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
+    p.add_argument("--overlap-chunks", type=int, default=0,
+                   help="row chunks of the overlapped Scheme II stages (0: the library's rule; 1: the four "
+                        "steps in order, one GEMM launch over all tiles)")
     return p.parse_args()
 
 
@@ -326,6 +329,8 @@ def run_ours(args, ws, rank, local):
     ex.set_stream(stream.cuda_stream)
     W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, M, N, K, S,
                                                                          materialize=args.materialize)
+    if args.overlap_chunks:
+        W.set_gemm_config(overlap_chunks=args.overlap_chunks)
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
 
@@ -417,7 +422,12 @@ def run_ours(args, ws, rank, local):
     # (Scheme II fused path; the library's default chunk rule) B's stats and
     # slicer plus per row chunk the A stats, A slicer, GEMM and CRT
     tiles = (M + 127) // 128
-    chunks = 4 if tiles >= 48 else (2 if tiles >= 8 else 1)
+    chunks = 2 if 8 <= tiles < 48 else 1
+    if args.overlap_chunks:
+        chunks = args.overlap_chunks
+    if chunks > 1:   # the library's split: q tiles per chunk, the last chunk possibly shorter
+        q = -(-tiles // min(chunks, 16, tiles))
+        chunks = -(-tiles // q)
     steps_kernels = 6 if (args.scheme != 2 or args.materialize or chunks == 1) else 2 + 4 * chunks
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

@@ -166,8 +166,8 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
  *   overlap_chunks  Scheme II fused path, calls without timings, one-CTA
  *                kernel: >= 2 splits the GEMM into that many row chunks and
  *                overlaps A's slicing and each chunk's reconstruction with
- *                the GEMM on two more streams; 1: the steps in order; 0: 4
- *                chunks from 48 row tiles of 128, 2 from 8, else 1.  Calls
+ *                the GEMM on two more streams; 1: the steps in order; 0: 2
+ *                chunks for 8 to 47 row tiles of 128, else 1.  Calls
  *                with timings, and the CTA-pair kernel, run the steps in order.
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */

@@ -516,12 +516,16 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
     const size_t M = ws->M, N = ws->N, K = ws->K;
 
     if (!timings && K && ws->fused && ws->cfg.cta_pair == 0) {
-        // Overlapped stages on the one-CTA kernel: measured 4% (8192^3, 4
-        // chunks) and 4.8% (4096^3, 2 chunks) faster than the steps in order.
+        // Overlapped stages on the one-CTA kernel, by default in 2 row chunks
+        // for 8..47 row tiles: +6% at 2048^3, +3.7% at 1024x1024x65536, +1.7%
+        // at 4096^3 over the steps in order.  From 48 tiles the GEMM dominates
+        // and a single full launch is faster per clock than chunk launches
+        // sharing the SMs with the slicer: at 8192^3 the steps in order run at
+        // 132.5 TFLOP/s against 127-129 with 2 to 4 chunks.
         int chunks = ws->cfg.overlap_chunks;
         if (chunks == 0) {
             const size_t tiles = (M + oza::kTileM - 1) / oza::kTileM;
-            chunks = tiles >= 48 ? 4 : (tiles >= 8 ? 2 : 1);
+            chunks = (tiles >= 8 && tiles < 48) ? 2 : 1;
         }
         if (chunks >= 2) {
             OZA_CUDA_TRY(overlap_init(ws), "oza_gemm: overlap streams");
