@@ -68,6 +68,23 @@ def parse():
     return p.parse_args()
 
 
+def launches_per_call(M, scheme, materialize, overlap_chunks=0):
+    """Kernels one device-buffer GEMM call launches (Scheme II/I, K > 0): the
+    four steps in order are 6 launches (row and column statistics, the two
+    slicers, the GEMM, the reconstruction).  The Scheme II fused path with
+    overlapped stages launches B's statistics and slicer once and, per row
+    chunk, A's statistics, A's slicer, a GEMM and a CRT.  The chunk rule is the
+    library's (oza_gemm): by default 2 chunks for 8..47 row tiles of 128, else
+    1; a requested count c becomes ceil(tiles / q) chunks of q = ceil(tiles /
+    min(c, 16, tiles)) tiles."""
+    tiles = (M + 127) // 128
+    chunks = overlap_chunks if overlap_chunks else (2 if 8 <= tiles < 48 else 1)
+    if chunks > 1:
+        q = -(-tiles // min(chunks, 16, tiles))
+        chunks = -(-tiles // q)
+    return 6 if (scheme != 2 or materialize or chunks == 1) else 2 + 4 * chunks
+
+
 def dims(args):
     if args.mnk:
         M, N, K = (int(x) for x in args.mnk.split(","))
@@ -418,17 +435,7 @@ def run_ours(args, ws, rank, local):
     traffic = load_traffic().get(workload(args)["workload"] + f"_S{S}")
     bytes_h2d = (M * K + K * N) * 8
     bytes_d2h = M * N * 8
-    # kernels per call: the four steps in order (6), or with overlapped stages
-    # (Scheme II fused path; the library's default chunk rule) B's stats and
-    # slicer plus per row chunk the A stats, A slicer, GEMM and CRT
-    tiles = (M + 127) // 128
-    chunks = 2 if 8 <= tiles < 48 else 1
-    if args.overlap_chunks:
-        chunks = args.overlap_chunks
-    if chunks > 1:   # the library's split: q tiles per chunk, the last chunk possibly shorter
-        q = -(-tiles // min(chunks, 16, tiles))
-        chunks = -(-tiles // q)
-    steps_kernels = 6 if (args.scheme != 2 or args.materialize or chunks == 1) else 2 + 4 * chunks
+    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
