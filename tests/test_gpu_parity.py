@@ -94,8 +94,8 @@ def test_exponent_edge_cases(executor, scheme, S):
     _check_all(got, ref)
 
 
-def test_config1_full_size_vs_oracle(executor):
-    """Config 1: 1024^3, phi = 0.5, Scheme II with 8 moduli, bit-exact end to end."""
+def test_1024_cubed_8_moduli_vs_oracle(executor):
+    """1024^3, phi = 0.5, Scheme II with 8 moduli, bit-exact end to end."""
     oz = _oz()
     from oracle import Oracle
     A = oz.generate_matrix(1024, 1024, 0.5, 42)

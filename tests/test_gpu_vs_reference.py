@@ -55,7 +55,7 @@ def test_scheme1_matches_reference_gpu(executor, S):
 
 
 def test_scheme2_4096_matches_reference_gpu(executor):
-    """A config-2 shape end to end: 4096^3, phi = 2, 16 moduli."""
+    """4096^3, phi = 2, 16 moduli, end to end."""
     oz = _oz()
     n = 4096
     A = oz.generate_matrix(n, n, 2.0, 42)
