@@ -62,13 +62,15 @@ def parse():
                    help="offered loads as fractions of the batched server's measured capacity")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
+    p.add_argument("--cta-pair", action="store_true",
+                   help="step 3 on the opt-in CTA-pair kernel (256x256 tiles on SM pairs); the steps then run in order")
     p.add_argument("--overlap-chunks", type=int, default=0,
                    help="row chunks of the overlapped Scheme II stages (0: the library's rule; 1: the four "
                         "steps in order, one GEMM launch over all tiles)")
     return p.parse_args()
 
 
-def launches_per_call(M, scheme, materialize, overlap_chunks=0):
+def launches_per_call(M, scheme, materialize, overlap_chunks=0, cta_pair=False):
     """Kernels one device-buffer GEMM call launches (Scheme II/I, K > 0): the
     four steps in order are 6 launches (row and column statistics, the two
     slicers, the GEMM, the reconstruction).  The Scheme II fused path with
@@ -76,13 +78,13 @@ def launches_per_call(M, scheme, materialize, overlap_chunks=0):
     chunk, A's statistics, A's slicer, a GEMM and a CRT.  The chunk rule is the
     library's (oza_gemm): by default 2 chunks for 8..47 row tiles of 128, else
     1; a requested count c becomes ceil(tiles / q) chunks of q = ceil(tiles /
-    min(c, 16, tiles)) tiles."""
+    min(c, 16, tiles)) tiles.  The CTA-pair kernel always runs the steps in order."""
     tiles = (M + 127) // 128
     chunks = overlap_chunks if overlap_chunks else (2 if 8 <= tiles < 48 else 1)
     if chunks > 1:
         q = -(-tiles // min(chunks, 16, tiles))
         chunks = -(-tiles // q)
-    return 6 if (scheme != 2 or materialize or chunks == 1) else 2 + 4 * chunks
+    return 6 if (scheme != 2 or materialize or cta_pair or chunks == 1) else 2 + 4 * chunks
 
 
 def dims(args):
@@ -95,14 +97,20 @@ def dims(args):
 def workload(args):
     M, N, K = dims(args)
     shape = f"{M}^3" if M == N == K else f"{M}x{N}x{K}"
-    return {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{shape}",
-            "M": M, "N": N, "K": K, "scheme": args.scheme,
-            "slices": args.slices, "phi": args.phi, "input_seeds": [42, 43],
-            "path": "materialized" if getattr(args, "materialize", False) else "fused",
-            "layout": "row-major fp64",
-            "l2": f"inputs ({(M * K + K * N) * 8 / 2**30:.2f} GiB) "
-                  + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
-                     "fit in L2: timings include L2 reuse")}
+    w = {"workload": f"scheme{'II' if args.scheme == 2 else 'I'}_dgemm_{shape}",
+         "M": M, "N": N, "K": K, "scheme": args.scheme,
+         "slices": args.slices, "phi": args.phi, "input_seeds": [42, 43],
+         "path": "materialized" if getattr(args, "materialize", False) else "fused",
+         "layout": "row-major fp64",
+         "l2": f"inputs ({(M * K + K * N) * 8 / 2**30:.2f} GiB) "
+               + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
+                  "fit in L2: timings include L2 reuse")}
+    # non-default step-3 settings are part of the workload's description
+    if getattr(args, "cta_pair", False):
+        w["gemm_kernel"] = "cta_pair"
+    if getattr(args, "overlap_chunks", 0):
+        w["overlap_chunks"] = args.overlap_chunks
+    return w
 
 
 def int8_ops(args):
@@ -346,8 +354,8 @@ def run_ours(args, ws, rank, local):
     ex.set_stream(stream.cuda_stream)
     W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, M, N, K, S,
                                                                          materialize=args.materialize)
-    if args.overlap_chunks:
-        W.set_gemm_config(overlap_chunks=args.overlap_chunks)
+    if args.overlap_chunks or args.cta_pair:
+        W.set_gemm_config(cta_pair=args.cta_pair, overlap_chunks=args.overlap_chunks)
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
 
@@ -435,7 +443,7 @@ def run_ours(args, ws, rank, local):
     traffic = load_traffic().get(workload(args)["workload"] + f"_S{S}")
     bytes_h2d = (M * K + K * N) * 8
     bytes_d2h = M * N * 8
-    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks)
+    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks, args.cta_pair)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
