@@ -157,6 +157,29 @@ def test_whole_pipeline_vs_reference_cpu(scheme, S):
     assert np.array_equal(bits(C), bits(C_ref))
 
 
+def _random_cases(n, seed):
+    rng = np.random.default_rng(seed)
+    for _ in range(n):
+        scheme = int(rng.integers(1, 3))
+        yield (scheme, int(rng.integers(1, 48)), int(rng.integers(1, 48)), int(rng.integers(1, 96)),
+               float(rng.choice([0.5, 1.0, 2.0, 4.0])), int(rng.integers(0, 2**31)),
+               int(rng.integers(1, 21)) if scheme == 2 else int(rng.integers(1, 13)))
+
+
+@needs_ref
+@pytest.mark.parametrize("scheme,M,N,K,phi,seed,S", list(_random_cases(40, 20261203)))
+def test_random_cases_vs_reference_cpu(scheme, M, N, K, phi, seed, S):
+    """Seeded random shapes (1..47 x 1..47 x 1..95), dynamic ranges, generator
+    seeds and slice counts: the oracle's C equals the reference pipeline's, bit
+    for bit, for both schemes."""
+    import ozablas_b200 as oz
+    A = oz.generate_matrix(M, K, phi, seed % 100000)
+    B = oz.generate_matrix(K, N, phi, seed % 100000 + 1)
+    C_ref, _ = Ref.cpu_pipeline(scheme, A, B, S)
+    C = (Oracle.scheme2 if scheme == 2 else Oracle.scheme1)(A, B, S)["C"]
+    assert np.array_equal(bits(C), bits(C_ref))
+
+
 def test_int8_gemm_exact():
     rng = np.random.default_rng(0)
     A = rng.integers(-128, 128, (33, 70)).astype(np.int8)
