@@ -26,7 +26,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -62,15 +61,13 @@ def parse():
                    help="offered loads as fractions of the batched server's measured capacity")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
-    p.add_argument("--cta-pair", action="store_true",
-                   help="step 3 on the opt-in CTA-pair kernel (256x256 tiles on SM pairs); the steps then run in order")
     p.add_argument("--overlap-chunks", type=int, default=0,
                    help="row chunks of the overlapped Scheme II stages (0: the library's rule; 1: the four "
                         "steps in order, one GEMM launch over all tiles)")
     return p.parse_args()
 
 
-def launches_per_call(M, scheme, materialize, overlap_chunks=0, cta_pair=False):
+def launches_per_call(M, scheme, materialize, overlap_chunks=0):
     """Kernels one device-buffer GEMM call launches (Scheme II/I, K > 0): the
     four steps in order are 6 launches (row and column statistics, the two
     slicers, the GEMM, the reconstruction).  The Scheme II fused path with
@@ -78,13 +75,13 @@ def launches_per_call(M, scheme, materialize, overlap_chunks=0, cta_pair=False):
     chunk, A's statistics, A's slicer, a GEMM and a CRT.  The chunk rule is the
     library's (oza_gemm): by default 2 chunks for 8..47 row tiles of 128, else
     1; a requested count c becomes ceil(tiles / q) chunks of q = ceil(tiles /
-    min(c, 16, tiles)) tiles.  The CTA-pair kernel always runs the steps in order."""
+    min(c, 16, tiles)) tiles."""
     tiles = (M + 127) // 128
     chunks = overlap_chunks if overlap_chunks else (2 if 8 <= tiles < 48 else 1)
     if chunks > 1:
         q = -(-tiles // min(chunks, 16, tiles))
         chunks = -(-tiles // q)
-    return 6 if (scheme != 2 or materialize or cta_pair or chunks == 1) else 2 + 4 * chunks
+    return 6 if (scheme != 2 or materialize or chunks == 1) else 2 + 4 * chunks
 
 
 def dims(args):
@@ -106,8 +103,6 @@ def workload(args):
                + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
                   "fit in L2: timings include L2 reuse")}
     # non-default step-3 settings are part of the workload's description
-    if getattr(args, "cta_pair", False):
-        w["gemm_kernel"] = "cta_pair"
     if getattr(args, "overlap_chunks", 0):
         w["overlap_chunks"] = args.overlap_chunks
     return w
@@ -159,8 +154,9 @@ def barrier(ws):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """SM clock and throttle reasons sampled every 10 ms (NVML) while the timed
-    region runs; falls back to nvidia-smi at 200 ms if NVML is unavailable."""
+    """SM clock, throttle reasons and power sampled every 10 ms through NVML
+    (pynvml) while the timed region runs; without NVML the summary reports
+    no samples."""
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4}
 
@@ -287,13 +283,16 @@ def cpu_reference_sample(args, A, B, steps=1, warmup=0):
 
 
 def run_reference_arm(args, ws, rank):
+    """The reference's CPU path alone: inputs from the reference's own
+    generator and its step 1/2/4 kernel source (both in oracle/_ref), an exact
+    CPU INT8 GEMM for step 3.  Nothing of this repository's library is loaded."""
     if rank != 0:
         return
     import numpy as np
-    import ozablas_b200 as oz
+    from oracle import Ref
     M, N, K = dims(args)
-    A = oz.generate_matrix(min(args.cpu_sample, M), K, args.phi, 42)
-    B = oz.generate_matrix(K, N, args.phi, 43)[:, :min(args.cpu_sample, N)]
+    A = Ref.generate_matrix(min(args.cpu_sample, M), K, args.phi, 42)
+    B = Ref.generate_matrix(K, N, args.phi, 43)[:, :min(args.cpu_sample, N)]
     res = cpu_reference_sample(args, A, np.ascontiguousarray(B), steps=args.steps, warmup=min(args.warmup, 1))
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["seconds_per_sample"] * 1e3, "higher_is_better": True,
@@ -354,8 +353,8 @@ def run_ours(args, ws, rank, local):
     ex.set_stream(stream.cuda_stream)
     W = (oz.WorkspaceScheme2 if args.scheme == 2 else oz.WorkspaceScheme1)(ex, M, N, K, S,
                                                                          materialize=args.materialize)
-    if args.overlap_chunks or args.cta_pair:
-        W.set_gemm_config(cta_pair=args.cta_pair, overlap_chunks=args.overlap_chunks)
+    if args.overlap_chunks:
+        W.set_gemm_config(overlap_chunks=args.overlap_chunks)
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
 
@@ -441,11 +440,11 @@ def run_ours(args, ws, rank, local):
     gemm_ms = step_ms["step3_ms"]
     achieved = int8_ops(args) / (gemm_ms * 1e-3) / 1e12
     # the ncu capture behind traffic.json is of the default step-3 settings
-    traffic = (None if (args.cta_pair or args.overlap_chunks)
+    traffic = (None if args.overlap_chunks
                else load_traffic().get(workload(args)["workload"] + f"_S{S}"))
     bytes_h2d = (M * K + K * N) * 8
     bytes_d2h = M * N * 8
-    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks, args.cta_pair)
+    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

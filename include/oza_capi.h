@@ -143,6 +143,19 @@ oza_status_t oza_ws_device_error(oza_ws_t ws, int* code);
 #define OZA_NOALLOC_SCRATCH_BYTES (64u << 20)
 oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_t N, size_t K, const double* A,
                               const double* B, double* C, void* stream);
+/* Device error word of the allocation-free GEMM on the current device: waits
+ * for `stream`, then *code = 1 if a bounded device-side wait expired in any
+ * oza_gemm_noalloc call since the previous query (its C is then not valid),
+ * else 0; the word is cleared.  Allocates nothing.  The array's address is
+ * looked up once per device and kept for the process: cudaDeviceReset between
+ * calls is not supported.  No counterpart in the reference. */
+oza_status_t oza_noalloc_device_error(void* stream, int* code);
+/* Self-test of that report, without a GPU fault: one kernel waits, through the
+ * GEMM kernels' bounded mbarrier wait, on a barrier nothing arrives on, with
+ * the array's error word as its error word; after limit_s (0 < limit_s <= 5)
+ * it gives up and sets the word, so the next oza_noalloc_device_error reports
+ * 1.  Synchronous on `stream`.  No counterpart in the reference. */
+oza_status_t oza_noalloc_selftest_wait_timeout(double limit_s, void* stream);
 
 /* Self-test of failure detection: one kernel waits, through the same bounded
  * mbarrier wait as the GEMM kernels, on a barrier that nothing arrives on.
@@ -154,27 +167,19 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
 
 /* ---- GEMM tuning ------------------------------------------------------------ */
 /* Step-3 kernel configuration of a workspace (0 fields: library defaults).
- *   pair_stages  TMA pipeline depth of the CTA-pair kernel, 4..7 (default 6)
- *   band         m-tiles per rasterisation band (default 16)
- *   cta_pair     1: the cluster-launched CTA-pair kernel (256 x 256 tiles on two
- *                SMs) instead of the default one-CTA kernel (128 x 256 tiles).
- *                Same results and, measured, the same speed within +-2%.  Do
- *                not run it concurrently with other kernels (another stream,
- *                another workspace): runs that overlapped it with other
- *                kernels stalled intermittently.
+ *   band         m-tiles (128 rows each) per rasterisation band of the GEMM's
+ *                output tiles (default 16)
  *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
- *   overlap_chunks  Scheme II fused path, calls without timings, one-CTA
- *                kernel: >= 2 splits the GEMM into that many row chunks and
- *                overlaps A's slicing and each chunk's reconstruction with
- *                the GEMM on two more streams; 1: the steps in order; 0: 2
- *                chunks for 8 to 47 row tiles of 128, else 1.  Calls
- *                with timings, and the CTA-pair kernel, run the steps in order.
+ *   overlap_chunks  Scheme II fused path, calls without timings: >= 2 splits
+ *                the GEMM into that many row chunks and overlaps A's slicing
+ *                and each chunk's reconstruction with the GEMM on two more
+ *                streams; 1: the steps in order; 0: 2 chunks for 8 to 47 row
+ *                tiles of 128, else 1.  Calls with timings run the steps in
+ *                order.
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
 typedef struct {
-    int pair_stages;
     int band;
-    int cta_pair;
     int wait_hint_ns;
     int overlap_chunks;
 } oza_gemm_config_t;

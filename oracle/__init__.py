@@ -88,6 +88,7 @@ _ref = _Lazy(REF_CPU_SO, {
     "ref_reconstruct1_group": (None, [_P, _P, _P, _I, _I, _I, _I, _P]),
     "ref_cpu_scheme2_gemm": (None, [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "ref_cpu_scheme1_gemm": (None, [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "ref_generate_matrix": (None, [_I, _I, ctypes.c_double, _I, _P]),
 })
 
 MAX_SLICES = 20
@@ -228,6 +229,13 @@ class Oracle:
 # ------------------------------------------------------------------ the reference's own kernels
 class Ref:
     """The reference's kernel source run on the host (oracle/_ref/libozaref_cpu.so)."""
+
+    @staticmethod
+    def generate_matrix(rows, cols, phi=0.5, seed=42):
+        """The reference's seeded generator (utils/matrix_gen.hpp:15-34)."""
+        out = np.empty((rows, cols), np.float64)
+        _ref.ref_generate_matrix(int(rows), int(cols), float(phi), int(seed), _p(out))
+        return out
 
     @staticmethod
     def tables():

@@ -62,8 +62,7 @@ class _WsInfo(ctypes.Structure):
 
 
 class _GemmConfig(ctypes.Structure):
-    _fields_ = [("pair_stages", ctypes.c_int), ("band", ctypes.c_int), ("cta_pair", ctypes.c_int),
-                ("wait_hint_ns", ctypes.c_int), ("overlap_chunks", ctypes.c_int)]
+    _fields_ = [("band", ctypes.c_int), ("wait_hint_ns", ctypes.c_int), ("overlap_chunks", ctypes.c_int)]
 
 
 class _GroupInfo(ctypes.Structure):
@@ -299,22 +298,17 @@ class _Workspace:
         _check(lib().oza_ws_device_error(self._h, ctypes.byref(c)))
         return c.value
 
-    def set_gemm_config(self, pair_stages: int = 0, band: int = 0, cta_pair: bool = False,
-                        wait_hint_ns: int = 0, overlap_chunks: int = 0) -> None:
+    def set_gemm_config(self, band: int = 0, wait_hint_ns: int = 0, overlap_chunks: int = 0) -> None:
         """Step-3 kernel configuration; results are bit-identical whatever it is
         (extension: oza_ws_set_gemm_config).
 
-        pair_stages    pipeline depth of the CTA-pair kernel, 4..7 (0: 6)
-        band           m-tiles per rasterisation band (0: 16)
-        cta_pair       run the opt-in CTA-pair kernel (256x256 tiles on SM
-                       pairs); the steps then run in order.  Do not overlap it
-                       with other kernels on other streams.
+        band           m-tiles (128 rows each) per rasterisation band (0: 16)
         wait_hint_ns   suspend-time hint of the kernel's mbarrier waits (0: poll)
         overlap_chunks Scheme II fused path without timings: >= 2 overlaps A's
                        slicing and the reconstruction with the GEMM in that many
                        row chunks; 1 runs the steps in order; 0 takes 2 chunks
                        for 8 to 47 row tiles of 128, else 1."""
-        cfg = _GemmConfig(int(pair_stages), int(band), int(bool(cta_pair)), int(wait_hint_ns), int(overlap_chunks))
+        cfg = _GemmConfig(int(band), int(wait_hint_ns), int(overlap_chunks))
         _check(lib().oza_ws_set_gemm_config(self._h, ctypes.byref(cfg)))
 
     def get_gemm_config(self) -> dict:

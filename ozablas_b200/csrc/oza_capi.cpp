@@ -57,6 +57,25 @@ oza_status_t cuda_fail(cudaError_t e, const char* what) {
 
 void oza::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
+oza_status_t oza::check_problem(const char* who, int scheme, size_t M, size_t N, size_t K, int slices) {
+    if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return fail(OZA_INVALID_ARG, "%s: unknown scheme %d", who, scheme);
+    // Messages of the reference's workspace constructors (src/core/workspace.cpp:24-25, 68-71).
+    if (scheme == OZA_SCHEME1 && slices < 1) return fail(OZA_INVALID_ARG, "OzaBLAS: Slices must be >= 1.");
+    if (scheme == OZA_SCHEME2 && (slices < 1 || slices > 20))
+        return fail(OZA_INVALID_ARG, "OzaBLAS: Scheme II supports between 1 and 20 slices.");
+    if (scheme == OZA_SCHEME1 && slices > 20)
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: Scheme I is built for at most 20 slices (got %d)", slices);
+    const size_t Mp = oza::round_up(M, oza::kTileM), Np = oza::round_up(N, oza::kTileN);
+    const size_t Kp = oza::round_up(K, oza::kTileK);
+    if ((double)slices * (double)Mp >= 2147483648.0 || (double)slices * (double)Np >= 2147483648.0 ||
+        Kp >= (1ull << 31))
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: problem too large for one workspace (M=%zu N=%zu K=%zu S=%d)", M, N, K,
+                    slices);
+    if (scheme == OZA_SCHEME2 && (double)K * 125.0 * 125.0 >= 2147483648.0)
+        return fail(OZA_UNSUPPORTED, "OzaBLAS: K=%zu exceeds the INT32-exact bound of Scheme II (K <= 137438)", K);
+    return OZA_OK;
+}
+
 
 struct oza_workspace {
     oza_executor* ex = nullptr;
@@ -73,11 +92,10 @@ struct oza_workspace {
     int32_t* ctc = nullptr;          // INT32 group planes (materialised / Scheme I)
     uint8_t* coef = nullptr;         // Scheme II CRT coefficient bytes [S][Mp][Np]
     bool fused = false;
-    bool pair = false;               // GEMM on CTA pairs (cta_group::2)
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     oza::PairList pairs{};
-    oza_gemm_config_t cfg{0, 0, 0, 0, 0};  // GEMM tuning (0: library defaults)
+    oza_gemm_config_t cfg{0, 0, 0};  // GEMM tuning (0: library defaults)
     // oza_gemm_host: device staging of A, B, C, copy streams and chunk events,
     // made on first use.
     struct HostPipe {
@@ -205,7 +223,6 @@ oza_status_t gemm_overlapped(oza_workspace* ws, const double* A, const double* B
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
-        plan.pair = false;
         plan.ctc = nullptr;
         plan.coef = ws->coef;
         plan.m_tile_begin = c * q;
@@ -366,13 +383,11 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     if (!out) return fail(OZA_INVALID_ARG, "oza_ws_create: null output handle");
     *out = nullptr;
     if (!ex) return fail(OZA_INVALID_ARG, "OzaBLAS: Executor cannot be null.");
-    if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return fail(OZA_INVALID_ARG, "OzaBLAS: unknown scheme %d", scheme);
-    if (scheme == OZA_SCHEME1 && slices < 1) return fail(OZA_INVALID_ARG, "OzaBLAS: Slices must be >= 1.");
-    if (scheme == OZA_SCHEME2 && (slices < 1 || slices > 20))
-        return fail(OZA_INVALID_ARG, "OzaBLAS: Scheme II supports between 1 and 20 slices.");
-    if (scheme == OZA_SCHEME1 && slices > 20)
-        return fail(OZA_UNSUPPORTED, "OzaBLAS: Scheme I is built for at most 20 slices (got %d)", slices);
     if (flags & ~OZA_WS_MATERIALIZE) return fail(OZA_INVALID_ARG, "oza_ws_create: unknown flags 0x%x", flags);
+    {
+        const oza_status_t chk = oza::check_problem("oza_ws_create", scheme, M, N, K, slices);
+        if (chk != OZA_OK) return chk;
+    }
 
     auto* ws = new (std::nothrow) oza_workspace();
     if (!ws) return fail(OZA_OOM, "oza_ws_create: host allocation failed");
@@ -382,9 +397,7 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     ws->M = M;
     ws->N = N;
     ws->K = K;
-    // CTA-pair kernel (256-row tiles) unless A has at most 128 rows.
-    ws->pair = M > (size_t)oza::kTileM;
-    ws->Mp = oza::round_up(M, ws->pair ? oza::kTileMPair : oza::kTileM);
+    ws->Mp = oza::round_up(M, oza::kTileM);
     ws->Np = oza::round_up(N, oza::kTileN);
     ws->Kp = oza::round_up(K, oza::kTileK);
     ws->groups = slices;
@@ -392,19 +405,6 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     ws->pairs = oza::make_pairs(scheme, slices);
     if (scheme == OZA_SCHEME2) ws->k_param = K ? oza_scheme2_k_param(slices, K) : 0;
     else ws->beta = K ? oza_scheme1_beta(K) : 1;
-
-    // TMA coordinates are 32-bit: plane rows must stay below 2^31.
-    if ((double)slices * (double)ws->Mp >= 2147483648.0 || (double)slices * (double)ws->Np >= 2147483648.0 ||
-        ws->Kp >= (1ull << 31)) {
-        delete ws;
-        return fail(OZA_UNSUPPORTED, "OzaBLAS: problem too large for one workspace (M=%zu N=%zu K=%zu S=%d)", M, N,
-                    K, slices);
-    }
-    // Scheme II products must stay exact in INT32: K * 125^2 < 2^31.
-    if (scheme == OZA_SCHEME2 && (double)K * 125.0 * 125.0 >= 2147483648.0) {
-        delete ws;
-        return fail(OZA_UNSUPPORTED, "OzaBLAS: K=%zu exceeds the INT32-exact bound of Scheme II (K <= 137438)", K);
-    }
 
     DeviceGuard g(ex->device);
     cudaError_t e = oza::upload_tables();
@@ -515,7 +515,7 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
     cudaStream_t st = ex->stream;
     const size_t M = ws->M, N = ws->N, K = ws->K;
 
-    if (!timings && K && ws->fused && ws->cfg.cta_pair == 0) {
+    if (!timings && K && ws->fused) {
         // Overlapped stages on the one-CTA kernel, by default in 2 row chunks
         // for 8..47 row tiles: +6% at 2048^3, +3.7% at 1024x1024x65536, +1.7%
         // at 4096^3 over the steps in order.  From 48 tiles the GEMM dominates
@@ -562,12 +562,9 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
-        plan.pair = ws->pair && ws->cfg.cta_pair != 0;
         plan.ctc = ws->ctc;
         plan.coef = ws->fused ? ws->coef : nullptr;
-        plan.stages = ws->cfg.pair_stages;
         plan.band = ws->cfg.band;
-        plan.one_cta = false;
         plan.wait_hint_ns = (uint32_t)ws->cfg.wait_hint_ns;
         OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[3], st), "CUDA: event record");
@@ -603,11 +600,9 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg) {
     if (!ws) return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: null workspace");
     if (!cfg) {
-        ws->cfg = oza_gemm_config_t{0, 0, 0, 0, 0};
+        ws->cfg = oza_gemm_config_t{0, 0, 0};
         return OZA_OK;
     }
-    if (cfg->pair_stages != 0 && (cfg->pair_stages < 4 || cfg->pair_stages > 7))
-        return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: pair_stages must be 0 or 4..7");
     if (cfg->band < 0 || cfg->band > 4096) return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: band out of range");
     if (cfg->overlap_chunks < 0 || cfg->overlap_chunks > oza_workspace::Overlap::kMaxChunks)
         return fail(OZA_INVALID_ARG, "oza_ws_set_gemm_config: overlap_chunks must be in [0, 16]");
@@ -629,8 +624,7 @@ oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, do
     const oza_gemm_config_t saved = ws->cfg;
     std::vector<oza_gemm_config_t> cand;
     const int bands[] = {8, 16, 32};
-    // One-CTA kernel only: the CTA-pair kernel stays an explicit opt-in.
-    for (int b : bands) cand.push_back(oza_gemm_config_t{0, b, 0, saved.wait_hint_ns, saved.overlap_chunks});
+    for (int b : bands) cand.push_back(oza_gemm_config_t{b, saved.wait_hint_ns, saved.overlap_chunks});
     float best_t = 1e30f;
     oza_gemm_config_t best_c = saved;
     for (const auto& c : cand) {
@@ -685,10 +679,7 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         // only) and reconstructed, and its rows of C go back while the next
         // chunk is computed.  Copies in and out run on their own streams.
         const int offset = ws->k_param;
-        const bool pair = ws->pair && ws->cfg.cta_pair != 0;
-        const size_t tile_m = pair ? oza::kTileMPair : oza::kTileM;
-        // Tiles that hold rows of A (Mp may be rounded further, to 256 rows,
-        // than the 128-row tiles of the one-CTA kernel need).
+        const size_t tile_m = oza::kTileM;
         const int mt_all = (int)((M + tile_m - 1) / tile_m);
         // 32 chunks: the exposed tail after the last A chunk lands (its
         // GEMM, CRT and copy-out) is 1/32 of the compute and of C.  At
@@ -732,14 +723,11 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
             plan.pairs = ws->pairs;
             plan.err = ws->err;
             plan.sms = ex->sms;
-            plan.pair = ws->pair;
             plan.ctc = nullptr;
             plan.coef = ws->coef;
             plan.m_tile_begin = c * q;
             plan.m_tile_count = std::min(q, mt_all - c * q);
-            plan.stages = ws->cfg.pair_stages;
             plan.band = ws->cfg.band;
-            plan.one_cta = !pair;
             plan.wait_hint_ns = (uint32_t)ws->cfg.wait_hint_ns;
             OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
             OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->shiftA + r0,

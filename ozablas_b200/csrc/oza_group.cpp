@@ -89,7 +89,6 @@ oza_status_t oza_group_create(oza_exec_t ex, int scheme, size_t count, const siz
                               const size_t* K, const int* slices, unsigned flags, oza_group_t* out) {
     if (!out) return gfail(OZA_INVALID_ARG, "oza_group_create: null output handle");
     *out = nullptr;
-    if (!ex) return gfail(OZA_INVALID_ARG, "oza_group_create: null executor");
     if (scheme != OZA_SCHEME2) return gfail(OZA_UNSUPPORTED, "oza_group_create: only Scheme II is grouped");
     if (count == 0 || !M || !N || !K || !slices) return gfail(OZA_INVALID_ARG, "oza_group_create: empty problem list");
     if (count > (1u << 20)) return gfail(OZA_INVALID_ARG, "oza_group_create: too many problems (%zu)", count);
@@ -101,7 +100,10 @@ oza_status_t oza_group_create(oza_exec_t ex, int scheme, size_t count, const siz
             return gfail(OZA_INVALID_ARG, "oza_group_create: problem %zu is too large", i);
         if (slices[i] < 1 || slices[i] > 20)
             return gfail(OZA_INVALID_ARG, "oza_group_create: problem %zu: Scheme II supports 1 to 20 slices", i);
+        const oza_status_t chk = oza::check_problem("oza_group_create", OZA_SCHEME2, M[i], N[i], K[i], slices[i]);
+        if (chk != OZA_OK) return chk;
     }
+    if (!ex) return gfail(OZA_INVALID_ARG, "oza_group_create: null executor");
     DeviceGuard dg(ex->device);
     if (!dg.ok) return gfail(OZA_CUDA_ERROR, "CUDA: Failed to set device %d", ex->device);
     G_TRY(oza::upload_tables(), "CUDA: constant tables");

@@ -1074,202 +1074,6 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_
 // Step 4: reconstruction
 // ---------------------------------------------------------------------------
 
-// ---------------------------------------------------------------------------
-// Step 3 on CTA pairs: tcgen05.mma.cta_group::2, 256 x 256 output tiles
-// ---------------------------------------------------------------------------
-// Same work units and epilogues as k_gemm_i8, but a cluster of two CTAs on two
-// SMs computes a 256 x 256 tile with M = 256 UMMAs: each CTA stages its own
-// 128 rows of A and its own 128-row half of B^T (16 + 16 KB per stage, 6
-// stages), so per SM the operand traffic per MAC is 2/3 of the one-CTA
-// 128 x 256 tile.  The even CTA issues the MMAs; TMA completions of both CTAs
-// are counted on its full barriers; MMA commits arrive on both CTAs'
-// barriers; both CTAs' epilogue warps release the accumulator on the even
-// CTA's acc_empty barrier.  Every TMA load is a plain load into this CTA.
-constexpr int kPairTileM = 256;                   // rows of C per CTA pair
-constexpr int kPairABytes = 128 * kTileK;         // this CTA's 128 rows of A
-constexpr int kPairBBytes = 128 * kTileK;         // this CTA's half of B^T
-constexpr int kPairStagesDefault = 6;
-template <int STAGES>
-constexpr int pair_smem() { return STAGES * (kPairABytes + kPairBBytes) + 1024 + 256; }
-static_assert(pair_smem<7>() <= 232448, "7 pair stages must fit in 227 KB of shared memory");
-
-template <int EPI, int kPairStages>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
-    k_gemm_i8_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                   const __grid_constant__ PairList pairs, const GemmArgs args) {
-    const uint32_t hint = args.wait_hint;
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = smem;
-    uint8_t* sB = smem + kPairStages * kPairABytes;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + kPairStages * kPairBBytes);
-    uint64_t* empty = full + kPairStages;
-    uint64_t* acc_full = empty + kPairStages;
-    uint64_t* acc_empty = acc_full + 2;
-    uint64_t* drain = acc_empty + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t rank = cluster_ctarank();
-    const bool leader = rank == 0;
-    const int pair_id = blockIdx.x >> 1, num_pairs = gridDim.x >> 1;
-    const int G = args.groups;
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < kPairStages; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
-        }
-        mbar_init(&acc_full[0], 1);
-        mbar_init(&acc_full[1], 1);
-        mbar_init(&acc_empty[0], 2 * kEpiWarps);
-        mbar_init(&acc_empty[1], 2 * kEpiWarps);
-        mbar_init(drain, 1);
-        *abort_flag = 0;
-        fence_barrier_init();
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
-    }
-    if (warp == 1) {
-        tmem_alloc_pair(tmem_slot, kTmemCols);
-        tmem_relinquish_pair();
-    }
-    tc_fence_before();
-    cluster_sync();   // barriers of both CTAs initialised before any remote signal
-    tc_fence_after();
-    const uint32_t tmem_base = *tmem_slot;
-    const int total_units = G * args.total_tiles;
-
-    if (warp == 0) {
-        // ---------------- TMA producer (both CTAs, one lane) ----------------
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            bool ok = true;
-            for (int u = pair_id; u < total_units && ok; u += num_pairs) {
-                const int grp = u / args.total_tiles;
-                int mt, nt;
-                tile_coords(u - grp * args.total_tiles, args, mt, nt);
-                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                    const int arow = (int)(pairs.a[p] * args.Mp + (long long)mt * kPairTileM + rank * 128);
-                    const int brow = (int)(pairs.b[p] * args.Np + (long long)nt * kTileN + rank * 128);
-                    for (int kb = 0; kb < args.k_blocks; ++kb) {
-                        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, args.err, hint)) {
-                            ok = false;
-                            break;
-                        }
-                        const uint32_t fbar = mapa_shared(smem_u32(&full[stage]), 0);
-                        if (leader) mbar_arrive_expect_tx(&full[stage], 2 * (kPairABytes + kPairBBytes));
-                        tma_load_2d_pair(sA + stage * kPairABytes, &tmA, fbar, kb * kTileK, arow);
-                        tma_load_2d_pair(sB + stage * kPairBBytes, &tmB, fbar, kb * kTileK, brow);
-                        if (++stage == kPairStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
-                    }
-                }
-            }
-            if (!ok && leader) {
-                // Let the copies of both CTAs land (the leader's full barriers count them).
-                volatile int no_abort = 0;
-                for (int j = 0; j < kPairStages; ++j) {
-                    int st = (stage + kPairStages - 1 - j) % kPairStages;
-                    uint32_t ph = (st < stage) ? phase : (phase ^ 1);
-                    mbar_wait(&full[st], ph, &no_abort, nullptr);
-                }
-            }
-        }
-        __syncwarp();
-    } else if (warp == 1) {
-        // ---------------- MMA issuer (even CTA, one lane) ----------------
-        if (leader && lane == 0) {
-            constexpr uint32_t idesc = umma_idesc_i8(kPairTileM, kTileN);
-            int stage = 0;
-            uint32_t phase = 0;
-            int local = 0;
-            bool ok = true;
-            for (int u = pair_id; u < total_units && ok; u += num_pairs, ++local) {
-                const int grp = u / args.total_tiles;
-                const int acc = local & 1;
-                const uint32_t acc_phase = (local >> 1) & 1;
-                if (!mbar_wait(&acc_empty[acc], acc_phase ^ 1, abort_flag, args.err, hint)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t d = tmem_base + acc * kAccCols;
-                uint32_t accumulate = 0;
-                for (int p = pairs.start[grp]; p < pairs.start[grp + 1] && ok; ++p) {
-                    for (int kb = 0; kb < args.k_blocks; ++kb) {
-                        if (!mbar_wait(&full[stage], phase, abort_flag, args.err, hint)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const uint64_t ad = umma_desc_sw128(smem_u32(sA + stage * kPairABytes));
-                        const uint64_t bd = umma_desc_sw128(smem_u32(sB + stage * kPairBBytes));
-#pragma unroll
-                        for (int k = 0; k < kTileK / 32; ++k) {
-                            umma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, accumulate);
-                            accumulate = 1;
-                        }
-                        umma_commit_pair(&empty[stage]);
-                        if (++stage == kPairStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
-                    }
-                }
-                if (!ok) break;
-                umma_commit_pair(&acc_full[acc]);
-            }
-            if (!ok) {
-                umma_commit_pair(drain);
-                volatile int no_abort = 0;
-                mbar_wait(drain, 0, &no_abort, nullptr);
-            }
-        }
-        __syncwarp();
-    } else {
-        // ---------------- epilogue (both CTAs, own TMEM) ----------------
-        const int q = warp & 3;
-        const int half = (warp - 2) >> 2;
-        const int row_local = q * 32 + lane;
-        const uint32_t empty_remote[2] = {mapa_shared(smem_u32(&acc_empty[0]), 0),
-                                          mapa_shared(smem_u32(&acc_empty[1]), 0)};
-        int local = 0;
-        bool ok = true;
-        for (int u = pair_id; u < total_units && ok; u += num_pairs, ++local) {
-            const int grp = u / args.total_tiles;
-            int mt, nt;
-            tile_coords(u - grp * args.total_tiles, args, mt, nt);
-            const long long row = (long long)mt * kPairTileM + rank * 128 + row_local;
-            const int acc = local & 1;
-            const uint32_t acc_phase = (local >> 1) & 1;
-            int w = 1;
-            if (lane == 0) w = mbar_wait(&acc_full[acc], acc_phase, abort_flag, args.err, hint);
-            if (__shfl_sync(0xFFFFFFFFu, w, 0) == 0) {
-                ok = false;
-                continue;
-            }
-            tc_fence_after();
-            const uint32_t taddr =
-                tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-            epilogue_unit<EPI>(args.ctc, args.coef, args.Mp, args.Np, args.S, taddr, row, grp, nt, half);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_cluster(empty_remote[acc]);
-        }
-    }
-
-    tc_fence_before();
-    cluster_sync();   // the peer's shared memory is read by the pair's MMAs until here
-    if (warp == 1) {
-        tc_fence_after();
-        tmem_dealloc_pair(tmem_base, kTmemCols);
-    }
-}
-
 // Scheme II step 4 from the coefficient byte planes [S][Mp][Np] written by the
 // GEMM epilogue: one thread per 4 consecutive columns of a row (a warp reads
 // 128 contiguous bytes per plane), exact CRT per element, FP64 C.  Few
@@ -1640,42 +1444,13 @@ static cudaError_t gemm_launch(const CUtensorMap& tmA, const CUtensorMap& tmB, c
     return cudaGetLastError();
 }
 
-template <int EPI, int STAGES>
-static cudaError_t gemm_launch_pair_s(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
-                                      const GemmArgs& a, int grid, cudaStream_t st) {
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_gemm_i8_pair<EPI, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    pair_smem<STAGES>());
-    });
-    if (attr != cudaSuccess) return attr;
-    k_gemm_i8_pair<EPI, STAGES><<<grid, kGemmThreads, pair_smem<STAGES>(), st>>>(tmA, tmB, pairs, a);
-    return cudaGetLastError();
-}
-
-template <int EPI>
-static cudaError_t gemm_launch_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
-                                    const GemmArgs& a, int grid, int stages, cudaStream_t st) {
-    switch (stages) {
-        case 4: return gemm_launch_pair_s<EPI, 4>(tmA, tmB, pairs, a, grid, st);
-        case 5: return gemm_launch_pair_s<EPI, 5>(tmA, tmB, pairs, a, grid, st);
-        case 6: return gemm_launch_pair_s<EPI, 6>(tmA, tmB, pairs, a, grid, st);
-        case 7: return gemm_launch_pair_s<EPI, 7>(tmA, tmB, pairs, a, grid, st);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
 cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
-    const bool pair = p.pair && !p.one_cta;
-    const int tile_m = pair ? kPairTileM : kTileM;
-    if (p.Mp % tile_m != 0) return cudaErrorInvalidValue;
+    if (p.Mp % kTileM != 0 || p.Np % kTileN != 0 || p.Kp % kTileK != 0) return cudaErrorInvalidValue;
     CUtensorMap tmA, tmB;
-    if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, 128)) return cudaErrorInvalidValue;
-    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, pair ? 128 : kTileN))
-        return cudaErrorInvalidValue;
+    if (!make_plane_map(&tmA, p.a_planes, (size_t)p.planes * p.Mp, p.Kp, kTileM)) return cudaErrorInvalidValue;
+    if (!make_plane_map(&tmB, p.b_planes, (size_t)p.planes * p.Np, p.Kp, kTileN)) return cudaErrorInvalidValue;
     GemmArgs a{};
-    const int all_m_tiles = (int)(p.Mp / tile_m);
+    const int all_m_tiles = (int)(p.Mp / kTileM);
     if (p.m_tile_begin < 0 || p.m_tile_count < 0 || p.m_tile_begin + p.m_tile_count > all_m_tiles)
         return cudaErrorInvalidValue;
     a.mt0 = p.m_tile_begin;
@@ -1683,7 +1458,7 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
     a.total_tiles = a.m_tiles * a.n_tiles;
-    // Default band measured: pair bands of 8 / 16 / 32 m-tiles read 9.5 / 7.0 / 11.0 GB at 8192^3 S=16.
+    // Default band: 16 m-tiles (2048 rows of A) per rasterisation band.
     const int band = p.band > 0 ? p.band : 16;
     a.band = a.m_tiles < band ? a.m_tiles : band;
     a.groups = p.pairs.num_groups;
@@ -1696,13 +1471,6 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.wait_hint = p.wait_hint_ns;
     const long long units = (long long)a.total_tiles * a.groups;
     if (units == 0) return cudaSuccess;
-    if (pair) {
-        const long long pairs_max = p.sms / 2;
-        const int grid = 2 * (int)(units < pairs_max ? units : pairs_max);
-        const int stages = p.stages > 0 ? p.stages : kPairStagesDefault;
-        return p.coef ? gemm_launch_pair<kEpiCoef>(tmA, tmB, p.pairs, a, grid, stages, st)
-                      : gemm_launch_pair<kEpiI32>(tmA, tmB, p.pairs, a, grid, stages, st);
-    }
     const int grid = (int)(units < p.sms ? units : p.sms);
     return p.coef ? gemm_launch<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
                   : gemm_launch<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);

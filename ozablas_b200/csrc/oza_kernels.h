@@ -12,8 +12,7 @@ constexpr int kMaxSlicesHost = 20;
 
 // Tile geometry of the INT8 tensor-core GEMM and the padding it imposes on
 // the workspace layouts.
-constexpr int kTileM = 128;   // rows of A per CTA tile (UMMA M, one-CTA variant)
-constexpr int kTileMPair = 256;   // rows of A per CTA-pair tile (cta_group::2 variant)
+constexpr int kTileM = 128;   // rows of A per CTA tile (UMMA M)
 constexpr int kTileN = 256;   // rows of B^T per CTA tile (UMMA N)
 constexpr int kTileK = 128;   // bytes of K per pipeline stage (one 128B swizzle row)
 
@@ -62,17 +61,13 @@ struct GemmPlan {
     PairList pairs;
     int* err;                 // device error word
     int sms;
-    bool pair;                // cta_group::2 kernel on CTA pairs (Mp multiple of 256)
     // epilogue output: INT32 group planes, or (Scheme II) CRT coefficient bytes
     int32_t* ctc;             // [groups][Mp][Np], used when coef == nullptr
     uint8_t* coef;            // [S][Mp][Np]
     int m_tile_begin = 0;     // restrict the launch to m-tiles [begin, begin + count) (count 0: to the end)
     int m_tile_count = 0;
-    // Tuning (0: defaults): pair-kernel pipeline stages (4..7), m-tiles per
-    // rasterisation band, and the one-CTA kernel in place of the pair kernel.
-    int stages = 0;
+    // Tuning (0: defaults): m-tiles per rasterisation band.
     int band = 0;
-    bool one_cta = false;
     uint32_t wait_hint_ns = 0;   // mbarrier suspend-time hint of the kernel's waits (0: poll)
 };
 cudaError_t launch_gemm_i8(const GemmPlan& plan, cudaStream_t st);

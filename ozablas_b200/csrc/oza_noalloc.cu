@@ -15,11 +15,18 @@
 // exits.  Host code cannot use the array's name as a device address, so the
 // first call on each device looks the address up with cudaGetSymbolAddress
 // (and uploads the CRT constant tables); that first call should therefore
-// happen before any stream capture.  All calls share the one array and it
-// keeps the previous call's contents: everything that must start at zero is
-// cleared on the stream.  Calls whose work overlaps on the GPU (different
-// streams, or host threads issuing concurrently) race on the array; issue
-// them on one stream or serialise them.
+// happen before any stream capture.  The looked-up address is cached per
+// device for the life of the process: a cudaDeviceReset between calls is not
+// supported.  All calls share the one array and it keeps the previous call's
+// contents: everything that must start at zero is cleared on the stream.
+// Calls whose work overlaps on the GPU (different streams, or host threads
+// issuing concurrently) race on the array; issue them on one stream or
+// serialise them.
+//
+// The first 256 bytes of the array hold the device error word (int at offset
+// 0): a kernel whose bounded wait expires sets it to 1.  No call clears it;
+// oza_noalloc_device_error() reads and clears it, so it reports every call
+// since the previous query.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -28,6 +35,7 @@
 #include <string>
 
 #include "oza_capi.h"
+#include "oza_internal.h"
 #include "oza_kernels.h"
 
 namespace {
@@ -88,10 +96,12 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return na_fail(OZA_INVALID_ARG, "oza_gemm_noalloc: unknown scheme");
     if (slices < 1 || slices > 20)
         return na_fail(OZA_INVALID_ARG, "oza_gemm_noalloc: slices must be between 1 and 20");
+    {
+        const oza_status_t chk = oza::check_problem("oza_gemm_noalloc", scheme, M, N, K, slices);
+        if (chk != OZA_OK) return chk;
+    }
     if (M == 0 || N == 0) return OZA_OK;
     if (!C || (K && (!A || !B))) return na_fail(OZA_INVALID_ARG, "oza_gemm_noalloc: null matrix pointer");
-    if (scheme == OZA_SCHEME2 && (double)K * 125.0 * 125.0 >= 2147483648.0)
-        return na_fail(OZA_UNSUPPORTED, "oza_gemm_noalloc: K exceeds the INT32-exact bound of Scheme II");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     int dev = 0;
@@ -107,8 +117,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     }
 
     // Same padded layouts as a workspace of oza_ws_create.
-    const bool pair = M > (size_t)oza::kTileM;
-    const size_t Mp = oza::round_up(M, pair ? oza::kTileMPair : oza::kTileM);
+    const size_t Mp = oza::round_up(M, oza::kTileM);
     const size_t Np = oza::round_up(N, oza::kTileN);
     const size_t Kp = oza::round_up(K, oza::kTileK);
     const size_t S = (size_t)slices;
@@ -116,7 +125,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     const size_t need_ap = align256(S * Mp * Kp + 16), need_bp = align256(S * Np * Kp + 16);
     const size_t need_out = align256(scheme == OZA_SCHEME2 ? S * Mp * Np + 16 : S * Mp * Np * 4 + 16);
     const size_t need = need_err + need_sa + need_sb + need_cm + need_ap + need_bp + need_out;
-    if (need > (size_t)OZA_NOALLOC_SCRATCH_BYTES || S * Mp >= (1ull << 31) || S * Np >= (1ull << 31)) {
+    if (need > (size_t)OZA_NOALLOC_SCRATCH_BYTES) {
         char msg[256];
         snprintf(msg, sizeof(msg),
                  "oza_gemm_noalloc: M=%zu N=%zu K=%zu S=%d needs %zu bytes of scratch, more than the built-in "
@@ -149,9 +158,10 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
         if (e__ != cudaSuccess)                                                                 \
             return na_fail(OZA_CUDA_ERROR, std::string("oza_gemm_noalloc: ") + what + ": " + cudaGetErrorString(e__)); \
     } while (0)
-    // The array keeps the last call's contents: the device error word starts at
-    // zero every call (the column maxima are zeroed by the statistics launch).
-    NA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st), "clearing the error word");
+    // The array keeps the last call's contents.  The column maxima are zeroed
+    // by the statistics launch; every other intermediate is fully rewritten
+    // before it is read; the error word is left as it is (sticky until
+    // oza_noalloc_device_error reads it).
     NA_TRY(oza::launch_stats_rows(A, M, K, k_param, shiftA, sms, st), "step 1 (rows)");
     NA_TRY(oza::launch_stats_cols(B, K, N, colmax, sms, st), "step 1 (columns)");
     NA_TRY(oza::launch_slice_rows(scheme, A, M, K, shiftA, slices, beta, k_param, aplanes, Mp, Kp, sms, st),
@@ -168,7 +178,6 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     plan.pairs = oza::make_pairs(scheme, slices);
     plan.err = err;
     plan.sms = sms;
-    plan.pair = false;
     plan.ctc = scheme == OZA_SCHEME1 ? reinterpret_cast<int32_t*>(out) : nullptr;
     plan.coef = scheme == OZA_SCHEME2 ? out : nullptr;
     NA_TRY(oza::launch_gemm_i8(plan, st), "step 3");
@@ -179,5 +188,46 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
                                         C, st),
                "step 4");
 #undef NA_TRY
+    return OZA_OK;
+}
+
+extern "C" oza_status_t oza_noalloc_device_error(void* stream, int* code) {
+    if (!code) return na_fail(OZA_INVALID_ARG, "oza_noalloc_device_error: null argument");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return na_fail(OZA_CUDA_ERROR, "oza_noalloc_device_error: no current device");
+    DeviceScratch* d = nullptr;
+    oza_status_t sst = setup_device(dev, &d);
+    if (sst != OZA_OK) return sst;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int host = 0;
+    cudaError_t e = cudaMemcpyAsync(&host, d->ptr, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d->ptr, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return na_fail(OZA_CUDA_ERROR, std::string("oza_noalloc_device_error: ") + cudaGetErrorString(e));
+    *code = host;
+    return OZA_OK;
+}
+
+extern "C" oza_status_t oza_noalloc_selftest_wait_timeout(double limit_s, void* stream) {
+    if (!(limit_s > 0.0) || limit_s > 5.0)
+        return na_fail(OZA_INVALID_ARG, "oza_noalloc_selftest_wait_timeout: limit in (0, 5] s");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return na_fail(OZA_CUDA_ERROR, "oza_noalloc_selftest_wait_timeout: no current device");
+    DeviceScratch* d = nullptr;
+    oza_status_t sst = setup_device(dev, &d);
+    if (sst != OZA_OK) return sst;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int* err = reinterpret_cast<int*>(d->ptr);
+    int* status = err + 1;   // inside the 256-byte error block
+    int host = 0;
+    cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = oza::launch_wait_probe(err, (unsigned long long)(limit_s * 1e9), status, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&host, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return na_fail(OZA_CUDA_ERROR, std::string("oza_noalloc_selftest_wait_timeout: ") + cudaGetErrorString(e));
+    if (host) return na_fail(OZA_CUDA_ERROR, "oza_noalloc_selftest_wait_timeout: the wait returned without an arrival");
     return OZA_OK;
 }

@@ -340,7 +340,6 @@ bool oza_server::launch() {
         g.pairs = oza::make_pairs(OZA_SCHEME2, p.S);
         g.err = err;
         g.sms = ex->sms;
-        g.pair = false;   // one-CTA kernel: batches on other slots run concurrently
         g.ctc = nullptr;
         g.coef = p.coef;
         e = cudaMemsetAsync(err, 0, sizeof(int), sl->st);
@@ -464,16 +463,22 @@ oza_status_t oza_server_create(oza_exec_t ex, const oza_server_config_t* cfg, oz
 
 size_t oza_server_request_bytes(size_t M, size_t N, size_t K, int slices) {
     if (M == 0 || N == 0 || K == 0 || slices < 1 || slices > 20) return 0;
+    if ((double)K * 125.0 * 125.0 >= 2147483648.0) return 0;   // beyond Scheme II's INT32-exact bound
     return WsLayout(M, N, K, slices).bytes;
 }
 
 oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, const double* A, const double* B,
                                double* C, int slices, uint64_t* id) {
-    if (!s || !id) return sfail(OZA_INVALID_ARG, "oza_server_submit: null argument");
+    // Sizes first (the same limits as oza_ws_create), then the handles.
     if (M == 0 || N == 0 || K == 0 || M > (1u << 30) || N > (1u << 30) || K > (1u << 30))
         return sfail(OZA_INVALID_ARG, "oza_server_submit: dimensions must be in [1, 2^30]");
-    if (!A || !B || !C) return sfail(OZA_INVALID_ARG, "oza_server_submit: null matrix pointer");
     if (slices < 1 || slices > 20) return sfail(OZA_INVALID_ARG, "oza_server_submit: slices must be in [1, 20]");
+    {
+        const oza_status_t chk = oza::check_problem("oza_server_submit", OZA_SCHEME2, M, N, K, slices);
+        if (chk != OZA_OK) return chk;
+    }
+    if (!s || !id) return sfail(OZA_INVALID_ARG, "oza_server_submit: null argument");
+    if (!A || !B || !C) return sfail(OZA_INVALID_ARG, "oza_server_submit: null matrix pointer");
     const size_t bytes = WsLayout(M, N, K, slices).bytes;
     // The batch block (column maxima, error word) and the batch's device
     // tables (work units: 16 bytes per S x 128 x 256 tile) come from the arena too.

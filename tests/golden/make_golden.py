@@ -13,7 +13,9 @@ the reference tree is absent.
     an exact INT8 GEMM for step 3, for Scheme II and Scheme I cases including
     exponent edge cases.
 
-Usage: python tests/golden/make_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_golden.py [--ref PATH]
+(PATH: a checkout of the reference tree; default $OZABLAS_REF, else a
+directory named "reference" beside this repository).
 """
 import argparse
 import os
@@ -117,7 +119,8 @@ def pipeline_fixture(name, A, B, scheme, S):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    default_ref = os.environ.get("OZABLAS_REF") or os.path.join(os.path.dirname(ROOT), "reference")
+    ap.add_argument("--ref", default=default_ref)
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}"], check=True)
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "ozablas_b200", "csrc")], check=True)

@@ -46,10 +46,3 @@ def test_unfused_paths_run_in_order(scheme, materialize):
     for M in (512, 4096, 8192):
         assert b.launches_per_call(M, scheme, materialize) == 6
         assert b.launches_per_call(M, scheme, materialize, 4) == 6
-
-
-def test_cta_pair_runs_in_order():
-    b = _bench()
-    for M in (1024, 4096, 8192):
-        for chunks in (0, 2, 4):
-            assert b.launches_per_call(M, 2, False, chunks, cta_pair=True) == 6

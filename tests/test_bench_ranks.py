@@ -46,3 +46,26 @@ def test_dist_max_over_ranks_gloo():
     for p in procs:
         p.join(timeout=60)
     assert res == {0: 3.0, 1: 3.0}
+
+
+def test_reference_arm_loads_only_the_checkers():
+    """The reference arm runs the reference's own code only: its inputs come
+    from the reference's generator and its steps from the reference's kernel
+    source, both in oracle/_ref; this repository's library is never loaded."""
+    import pytest
+    sys.path.insert(0, ROOT)
+    from oracle import ref_available
+    if not ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    code = (
+        "import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--size', '256', '--slices', '4',"
+        " '--steps', '1', '--warmup', '0', '--cpu-sample', '64']\n"
+        "import runpy; runpy.run_path('bench.py', run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED', json.dumps({'pkg': 'ozablas_b200' in sys.modules, 'lib': 'liboza_b200' in maps,"
+        " 'ref': 'libozaref_cpu' in maps}))\n")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="2")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    loaded = json.loads(out.stdout.split("LOADED", 1)[1])
+    assert loaded == {"pkg": False, "lib": False, "ref": True}

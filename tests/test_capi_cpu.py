@@ -76,6 +76,23 @@ def test_generator_matches_reference_fixture():
         assert np.array_equal(got.view(np.int64), g[f"case{i}"].view(np.int64))
 
 
+def test_reference_generator_build_matches_fixture_and_library():
+    """The reference's own generator compiled into oracle/_ref (the bench's
+    reference arm draws its inputs with it) gives the fixture's values and
+    this library's, bit for bit."""
+    from oracle import Ref, ref_available
+    if not ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    g = np.load(os.path.join(GOLDEN, "generator.npz"))
+    for i in range(4):
+        r, c, phi, seed = g[f"params{i}"]
+        got = Ref.generate_matrix(int(r), int(c), float(phi), int(seed))
+        assert np.array_equal(got.view(np.int64), g[f"case{i}"].view(np.int64))
+    for r, c, phi, seed in [(64, 8192, 0.5, 42), (8192, 64, 0.5, 43), (33, 77, 4.0, 9)]:
+        a, b = Ref.generate_matrix(r, c, phi, seed), oz.generate_matrix(r, c, phi, seed)
+        assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
 @pytest.mark.parametrize("K", [1, 5, 64, 1000, 1024, 8192, 65536, 100000])
 def test_host_scheme_parameters_match_oracle(K):
     from oracle import Oracle
@@ -127,6 +144,47 @@ def test_group_api_rejects_bad_arguments_without_a_device():
     assert L.oza_group_create(None, 2, 1, one, one, one, s, 0, ctypes.byref(h)) == oz.OZA_INVALID_ARG
     assert L.oza_group_gemm(None, None, None, None, None) == oz.OZA_INVALID_ARG
     assert L.oza_group_destroy(None) == oz.OZA_OK
+
+
+@pytest.mark.parametrize("K,want", [(137438, "ok"), (137439, "unsupported")])
+def test_scheme2_int32_bound_enforced_by_every_entry_point(K, want):
+    """Scheme II's INT32-exact bound (K * 125^2 < 2^31, K <= 137438) and the
+    slice range are enforced by one shared check in every GEMM entry point:
+    a request beyond the bound is refused with OZA_UNSUPPORTED before any
+    device work, in the workspace path, the allocation-free path, the grouped
+    GEMM and the request loop.  (At the bound itself the calls reach their
+    next check: a missing executor, server or matrix pointer.)"""
+    L = oz.lib()
+    h = ctypes.c_void_p()
+    one = lambda v: (ctypes.c_size_t * 1)(v)   # noqa: E731
+    s = (ctypes.c_int * 1)(4)
+    rid = ctypes.c_uint64()
+    results = {
+        "group": L.oza_group_create(None, 2, 1, one(8), one(8), one(K), s, 0, ctypes.byref(h)),
+        "server": L.oza_server_submit(None, 8, 8, K, None, None, None, 4, ctypes.byref(rid)),
+        "noalloc": L.oza_gemm_noalloc(2, 4, 8, 8, K, None, None, None, None),
+    }
+    for name, st in results.items():
+        if want == "unsupported":
+            assert st == oz.OZA_UNSUPPORTED, name
+        else:
+            assert st == oz.OZA_INVALID_ARG, name   # past the size check, stopped at a null handle/pointer
+    assert (oz.Server.request_bytes(8, 8, K, 4) == 0) == (want == "unsupported")
+    if want == "unsupported":
+        assert "INT32-exact" in L.oza_last_error_string().decode()
+
+
+def test_shared_check_rejects_slice_counts_and_tma_extents():
+    L = oz.lib()
+    # slices outside 1..20 (Scheme II: the reference's message)
+    assert L.oza_gemm_noalloc(2, 21, 8, 8, 8, None, None, None, None) == oz.OZA_INVALID_ARG
+    h = ctypes.c_void_p()
+    one = lambda v: (ctypes.c_size_t * 1)(v)   # noqa: E731
+    assert L.oza_group_create(None, 2, 1, one(8), one(8), one(8), (ctypes.c_int * 1)(0), 0,
+                              ctypes.byref(h)) == oz.OZA_INVALID_ARG
+    # 20 planes of 2^27 rows: S * Mp reaches 2^31, beyond 32-bit TMA coordinates
+    assert L.oza_gemm_noalloc(1, 20, 1 << 27, 8, 8, None, None, None, None) == oz.OZA_UNSUPPORTED
+    assert "too large" in L.oza_last_error_string().decode()
 
 
 def test_server_api_without_a_device():

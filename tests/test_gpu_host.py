@@ -67,17 +67,15 @@ def test_host_gemm_rejects_device_and_misshaped_buffers(executor):
 
 @pytest.mark.parametrize("M,N,K,S", [(257, 255, 129, 19), (2304, 512, 300, 12), (700, 130, 96, 8),
                                      (4500, 136, 96, 8), (8300, 72, 40, 5)])
-@pytest.mark.parametrize("cta_pair", [False, True])
-def test_host_gemm_both_kernels(executor, M, N, K, S, cta_pair):
-    """Row chunks of 128 (one-CTA kernel) and 256 rows (CTA-pair kernel) both
-    cover M exactly, also when M is not a multiple of the tile and when a
-    chunk holds several tiles (more tiles than the 32 chunks)."""
+def test_host_gemm_row_chunks_cover_m(executor, M, N, K, S):
+    """Row chunks of 128-row tiles cover M exactly, also when M is not a
+    multiple of the tile and when a chunk holds several tiles (more tiles
+    than the 32 chunks)."""
     import torch
     A = oz.generate_matrix(M, K, 0.5, 13)
     B = oz.generate_matrix(K, N, 0.5, 14)
     want = _device_result(executor, 2, A, B, S)
     ws = oz.WorkspaceScheme2(executor, M, N, K, S)
-    ws.set_gemm_config(cta_pair=cta_pair)
     hC = torch.full((M, N), float("nan"), dtype=torch.float64).pin_memory()
     oz.ozaki_gemm_host(ws, torch.from_numpy(A).pin_memory(), torch.from_numpy(B).pin_memory(), hC)
     assert np.array_equal(hC.numpy().view(np.int64), want.view(np.int64))

@@ -73,3 +73,32 @@ def test_noalloc_rejects_problems_beyond_the_array(executor):
     assert rc == oz.OZA_UNSUPPORTED
     assert b"bytes of scratch" in L.oza_last_error_string()
     assert fn(3, 16, 8, 8, 8, A.data_ptr(), A.data_ptr(), C.data_ptr(), None) == oz.OZA_INVALID_ARG
+    # Scheme II's INT32-exact bound is checked before any scratch sizing
+    assert fn(2, 4, 8, 8, 137439, A.data_ptr(), A.data_ptr(), C.data_ptr(), None) == oz.OZA_UNSUPPORTED
+    assert b"INT32-exact" in L.oza_last_error_string()
+
+
+def test_noalloc_reports_an_expired_wait(executor):
+    """A bounded wait that expires inside a kernel must not pass silently: the
+    self-test makes one wait run out on the array's error word (no GPU fault),
+    the query then reports 1 and clears the word, and after a clean call it
+    reports 0."""
+    import torch
+    oz, L, fn = _noalloc()
+    q = L.oza_noalloc_device_error
+    q.restype, q.argtypes = ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    probe = L.oza_noalloc_selftest_wait_timeout
+    probe.restype, probe.argtypes = ctypes.c_int, [ctypes.c_double, ctypes.c_void_p]
+    _setup_call(oz, fn)
+    code = ctypes.c_int(-1)
+    assert q(None, ctypes.byref(code)) == 0   # start from a cleared word
+    assert probe(0.2, None) == 0, L.oza_last_error_string()
+    assert q(None, ctypes.byref(code)) == 0 and code.value == 1
+    assert q(None, ctypes.byref(code)) == 0 and code.value == 0   # the query cleared it
+    M, N, K = 200, 150, 300
+    A = torch.from_numpy(oz.generate_matrix(M, K, 1.0, 1)).cuda()
+    B = torch.from_numpy(oz.generate_matrix(K, N, 1.0, 2)).cuda()
+    C = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    assert fn(2, 12, M, N, K, A.data_ptr(), B.data_ptr(), C.data_ptr(), None) == 0
+    assert q(None, ctypes.byref(code)) == 0 and code.value == 0
+    assert bool(torch.isfinite(C).all())
