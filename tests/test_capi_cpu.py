@@ -227,3 +227,29 @@ def test_slices_for_target_is_a_monotone_lookup():
 def test_selftest_rejects_null_executor():
     code = ctypes.c_int()
     assert oz.lib().oza_selftest_wait_timeout(None, 0.1, ctypes.byref(code), None) == oz.OZA_INVALID_ARG
+
+
+HARNESSES = ["precision_benchmarks/01_ozaki_scheme2_example.cpp", "precision_benchmarks/02_ozaki_scheme2_fp128_benchmark.cpp",
+             "precision_benchmarks/03_ozaki_scheme1_example.cpp", "precision_benchmarks/04_ozaki_scheme1_fp128_benchmark.cpp",
+             "performance_benchmarks/01_ozaki_scheme1_2_raw_performance.cpp",
+             "performance_benchmarks/02_ozaki_scheme2_pipeline_steps.cpp",
+             "performance_benchmarks/03_ozaki_scheme1_pipeline_steps.cpp"]
+
+
+@pytest.mark.parametrize("src", HARNESSES)
+def test_reference_harnesses_build_against_drop_in_headers(src, tmp_path):
+    """Every benchmark and example program of the reference compiles, unmodified,
+    against this repository's headers (include/ozablas/...) with
+    -DOZA_BUILD_CUDA and links against liboza_b200.so: the reference's whole
+    public API surface that its own programs use is present here."""
+    import __graft_entry__
+    ref = __graft_entry__.reference_tree()
+    if ref is None:
+        pytest.skip("reference tree not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "harness"
+    subprocess.run(["/usr/bin/g++", "-std=c++20", "-O0", "-fopenmp", "-DOZA_BUILD_CUDA", f"-I{root}/include",
+                    f"-I{ref}/utils", "-I/usr/local/cuda/include", os.path.join(ref, src), "-o", str(exe),
+                    f"-L{root}/ozablas_b200", "-loza_b200", "-L/usr/local/cuda/lib64", "-lcublas"], check=True)
+    syms = subprocess.run(["nm", "-u", "-C", str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "ozablas::CudaExecutor::CudaExecutor(int)" in syms
