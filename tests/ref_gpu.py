@@ -65,3 +65,33 @@ def run(executor, scheme, A, B, S):
         return out
     finally:
         L.refgpu_ws_destroy(h)
+
+
+def run_device(executor, scheme, dA, dB, S):
+    """The reference pipeline on device inputs (CUDA float64 tensors); returns
+    C and the intermediates as CUDA tensors in the reference's layouts, copied
+    out of its workspace before that is freed (for sizes where host copies
+    would be slow)."""
+    import torch
+    L = lib()
+    M, K = dA.shape
+    N = dB.shape[1]
+    h = L.refgpu_ws_create(scheme, M, N, K, S)
+    assert h, "reference workspace allocation failed"
+    try:
+        dC = torch.empty(M, N, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert L.refgpu_gemm(h, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+
+        def grab(which, shape, dtype):
+            t = torch.empty(shape, dtype=dtype, device="cuda")
+            executor.copy_device_to_device(t.data_ptr(), L.refgpu_ws_ptr(h, which), t.numel() * t.element_size())
+            return t
+
+        G = S if scheme == 2 else 1
+        return dict(C=dC, shift_A=grab(0, (M,), torch.int32), shift_B=grab(1, (N,), torch.int32),
+                    A_slices=grab(2, (S, M, K), torch.int8), B_slices=grab(3, (S, K, N), torch.int8),
+                    C_tc=grab(4, (G, M, N), torch.int32))
+    finally:
+        L.refgpu_ws_destroy(h)
