@@ -578,7 +578,7 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
                          "step4 crt");
         } else {
             OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->beta, ws->shiftA,
-                                                  ws->shiftB, C, st),
+                                                  ws->shiftB, C, ex->sms, st),
                          "step4 sum");
         }
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[4], st), "CUDA: event record");

@@ -34,17 +34,28 @@ struct ModConst {
     uint32_t dig[4];
 };
 
-// Scheme II CRT table for one slice count S.
+// Scheme II CRT table for one slice count S.  T = sum_s c_s (M / m_s), with
+// c_s = ((C_s mod m_s) inv_s) mod m_s the one-byte CRT coefficients, is formed
+// three residues at a time: for a triple (a, b, c) of moduli,
+//   c_a M/m_a + c_b M/m_b + c_c M/m_c = d (M / (m_a m_b m_c)),
+//   d = c_a m_b m_c + c_b m_a m_c + c_c m_a m_b < 3 * 250 * 2^16 < 2^26,
+// so each triple costs one 32 x 128-bit product instead of three.  The last
+// S mod 3 residues form a pair (d = c_a m_b + c_b m_a) or stay single.
 struct CrtTable {
     uint32_t M[5];            // M = prod m_i as 5 x 32-bit limbs (M < 2^153)
     uint32_t Mhalf[5];        // floor(M / 2)
     uint32_t P[kMaxSlices][5];  // M / m_i
     uint32_t inv[kMaxSlices];   // (M / m_i)^-1 mod m_i
     uint32_t c16inv[kMaxSlices];  // (2^16 * inv_i) mod m_i
-    uint32_t recip24[kMaxSlices]; // floor(2^24 / m_i), for the quotient estimate
-    // Residue pairs (2p, 2p+1): c_a M/m_a + c_b M/m_b = (c_a m_b + c_b m_a) M/(m_a m_b)
-    uint32_t PP[kMaxSlices / 2][5];      // M / (m_2p m_2p+1)
-    uint32_t precip24[kMaxSlices / 2];   // floor(2^24 / (m_2p m_2p+1))
+    unsigned long long recip48[kMaxSlices];   // floor(2^48 / m_i), for the quotient estimate
+    // Triples (3t, 3t+1, 3t+2), t < S / 3
+    uint32_t TP[kMaxSlices / 3][5];           // M / (m_a m_b m_c)
+    uint32_t tk[kMaxSlices / 3];              // (m_b m_c) | (m_a m_c) << 16: dp2a weights of c_a, c_b
+    uint32_t tab[kMaxSlices / 3];             // m_a m_b: weight of c_c
+    unsigned long long trecip48[kMaxSlices / 3];  // floor(2^48 / (m_a m_b m_c))
+    // The last two residues (S - 2, S - 1) when S mod 3 == 2
+    uint32_t DP[5];                           // M / (m_{S-2} m_{S-1})
+    unsigned long long drecip48;              // floor(2^48 / (m_{S-2} m_{S-1}))
     int nlimbs;                   // limbs of M that can be nonzero
 };
 

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -128,18 +129,24 @@ cudaError_t upload_tables() {
         for (int l = 0; l < 5; ++l)
             if (M.w[l]) nl = l + 1;
         t.nlimbs = nl;
+        // M / (product of the moduli in `skip`) as limbs
+        auto cofactor = [&](std::initializer_list<int> skip, uint32_t (&out)[5]) {
+            Big P = big_from(1);
+            for (int j = 0; j < S; ++j)
+                if (std::find(skip.begin(), skip.end(), j) == skip.end()) P = big_mul_small(P, kModuli[j]);
+            for (int l = 0; l < 5; ++l) out[l] = P.w[l];
+        };
         for (int i = 0; i < kMaxSlices; ++i) {
             if (i >= S) {
                 for (int l = 0; l < 5; ++l) t.P[i][l] = 0;
                 t.inv[i] = 0;
                 t.c16inv[i] = 0;
-                t.recip24[i] = 0;
+                t.recip48[i] = 0;
                 continue;
             }
-            Big P = big_from(1);
-            for (int j = 0; j < S; ++j)
-                if (j != i) P = big_mul_small(P, kModuli[j]);
-            for (int l = 0; l < 5; ++l) t.P[i][l] = P.w[l];
+            cofactor({i}, t.P[i]);
+            Big P;
+            for (int l = 0; l < 5; ++l) P.w[l] = t.P[i][l];
             uint32_t m = kModuli[i], r = big_mod_small(P, m), inv = 0;
             for (uint32_t c = 1; c < m; ++c)
                 if ((uint64_t)r * c % m == 1) {
@@ -148,18 +155,25 @@ cudaError_t upload_tables() {
                 }
             t.inv[i] = inv;
             t.c16inv[i] = (uint32_t)((65536ull * inv) % m);
-            t.recip24[i] = (uint32_t)((1u << 24) / m);
+            t.recip48[i] = (1ull << 48) / m;
         }
-        for (int p = 0; p < kMaxSlices / 2; ++p) {
-            const int a = 2 * p, b = 2 * p + 1;
-            for (int l = 0; l < 5; ++l) t.PP[p][l] = 0;
-            t.precip24[p] = 0;
-            if (b >= S) continue;
-            Big P = big_from(1);
-            for (int j = 0; j < S; ++j)
-                if (j != a && j != b) P = big_mul_small(P, kModuli[j]);
-            for (int l = 0; l < 5; ++l) t.PP[p][l] = P.w[l];
-            t.precip24[p] = (uint32_t)((1u << 24) / (kModuli[a] * kModuli[b]));
+        for (int q = 0; q < kMaxSlices / 3; ++q) {
+            const int a = 3 * q, b = a + 1, c = a + 2;
+            for (int l = 0; l < 5; ++l) t.TP[q][l] = 0;
+            t.tk[q] = t.tab[q] = 0;
+            t.trecip48[q] = 0;
+            if (c >= S) continue;
+            const uint64_t ma = kModuli[a], mb = kModuli[b], mc = kModuli[c];
+            cofactor({a, b, c}, t.TP[q]);
+            t.tk[q] = (uint32_t)(mb * mc) | ((uint32_t)(ma * mc) << 16);
+            t.tab[q] = (uint32_t)(ma * mb);
+            t.trecip48[q] = (1ull << 48) / (ma * mb * mc);
+        }
+        for (int l = 0; l < 5; ++l) t.DP[l] = 0;
+        t.drecip48 = 0;
+        if (S % 3 == 2) {
+            cofactor({S - 2, S - 1}, t.DP);
+            t.drecip48 = (1ull << 48) / ((uint64_t)kModuli[S - 2] * kModuli[S - 1]);
         }
     }
     e = cudaMemcpyToSymbol(c_mod, mc, sizeof(mc));
@@ -580,30 +594,26 @@ __device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t ma
 }
 
 // Running state of one element: T = sum c_s * (M / m_s) as NL 64-bit column
-// sums of 32-bit limb products (each below 2^45), and a fixed-point estimate
-// of T / M (units of 2^-24, an underestimate by at most 0.07).
+// sums of 32-bit limb products (each product below 2^58, at most 20 of them),
+// and a fixed-point estimate of T / M in units of 2^-48 (an underestimate by
+// less than 2^-18).
 template <int NL>
 struct CrtAcc {
     unsigned long long a[NL];
-    uint32_t q;
+    unsigned long long q;
     __device__ __forceinline__ void zero() {
 #pragma unroll
         for (int l = 0; l < NL; ++l) a[l] = 0ull;
-        q = 0;
+        q = 0ull;
+    }
+    // d * W where W = M / (product of the moduli d stands for), recip = floor(2^48 / that product)
+    __device__ __forceinline__ void add(const uint32_t (&W)[5], unsigned long long recip, uint32_t d) {
+#pragma unroll
+        for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)d * W[l];
+        q += (unsigned long long)d * recip;
     }
     // one residue s with coefficient c < m_s
-    __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) {
-#pragma unroll
-        for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)c * T.P[s][l];
-        q += c * T.recip24[s];
-    }
-    // residues 2p, 2p+1 with coefficients ca, cb: d = ca m_b + cb m_a < 2^17
-    __device__ __forceinline__ void add_pair(const CrtTable& T, int p, uint32_t ca, uint32_t cb) {
-        const uint32_t d = ca * c_mod[2 * p + 1].m + cb * c_mod[2 * p].m;
-#pragma unroll
-        for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)d * T.PP[p][l];
-        q += d * T.precip24[p];
-    }
+    __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) { add(T.P[s], T.recip48[s], c); }
 };
 
 // r = x - y over N 32-bit limbs.  The whole borrow chain is one asm block: the
@@ -656,7 +666,7 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
     t[NL] = (uint32_t)carry;
     // nearest quotient: the estimate is q* or q* - 1, so V = T - q M is either
     // the answer or the answer + M (then V >= floor(M/2)).
-    const uint32_t q = (acc.q + (1u << 23)) >> 24;
+    const uint32_t q = (uint32_t)((acc.q + (1ull << 47)) >> 48);
     uint32_t qm[L];
     {
         unsigned long long c = 0;
@@ -713,13 +723,15 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
 // drift across all S planes and re-read them from HBM (4.6x at 8192^3, S=16).
 //   warp 0      TMA producer (4-stage ring of A 128x128 + B^T 256x128 int8 tiles)
 //   warp 1      TMEM allocation, UMMA issue (one elected lane)
-//   warps 2..9  epilogue; warp w reads TMEM lanes 32 (w % 4).. and column half (w - 2) / 4
+//   warps 2..5  epilogue; warp w reads TMEM lanes 32 (w % 4).. (its lane
+//               quadrant), all 256 columns in two halves.  Four warps measured
+//               1-2% faster GEMMs than eight (one warp per quadrant and half).
 // Epilogues: kEpiI32 writes the INT32 group planes; kEpiCoef (Scheme II)
 // reduces each residue product to its one-byte CRT coefficient and writes the
 // byte planes, which k_crt_coef turns into FP64 C (a quarter of the INT32
-// traffic, and the multiword CRT runs at full occupancy instead of in the 8
+// traffic, and the multiword CRT runs at full occupancy instead of in the
 // epilogue warps, where it would stall the MMA pipeline).
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 4;
 constexpr int kGemmThreads = 64 + 32 * kEpiWarps;
 constexpr int kStages = 4;
 constexpr int kABytes = kTileM * kTileK;   // 16 KB per stage
@@ -1022,7 +1034,6 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3;                 // TMEM lane quadrant this warp may access
-        const int half = (warp - 2) >> 2;       // column half of the tile
         const int row_local = q * 32 + lane;
         int local = 0;
         bool ok = true;
@@ -1039,9 +1050,11 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
                 continue;
             }
             tc_fence_after();
-            const uint32_t taddr =
-                tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-            epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, half);
+            for (int half = 0; half < 2; ++half) {
+                const uint32_t taddr =
+                    tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
+                epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, half);
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -1076,16 +1089,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_
 
 // Scheme II step 4 from the coefficient byte planes [S][Mp][Np] written by the
 // GEMM epilogue: one thread per 4 consecutive columns of a row (a warp reads
-// 128 contiguous bytes per plane), exact CRT per element, FP64 C.  Few
-// registers per thread, so the multiword arithmetic runs at full occupancy;
-// with S fixed at compile time the table constants are instruction operands
-// and the S loads are issued together.
+// 128 contiguous bytes per plane), exact CRT per element, FP64 C.  Residues
+// are combined three at a time (CrtTable): the bytes of moduli a and b are
+// interleaved with one byte permute per 2 elements and weighted by m_b m_c and
+// m_a m_c in one dp2a; c_c m_a m_b is its accumulator.  With S fixed at
+// compile time the table constants are instruction operands and the S loads
+// are issued together.
 template <int S>
 __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef, long long Np, long long N,
                                                size_t plane, const int32_t* __restrict__ sA,
                                                const int32_t* __restrict__ sB, double* __restrict__ C,
                                                long long chunks, long long id) {
     constexpr int NL = (S + 3) / 4;   // 32-bit limbs of M
+    constexpr int NT = S / 3;         // residue triples
     const CrtTable& T = c_crt[S - 1];
     const long long i = id / chunks, j0 = (id - i * chunks) << 2;
     const uint8_t* src = coef + (size_t)i * Np + j0;
@@ -1096,14 +1112,30 @@ __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef,
 #pragma unroll
     for (int e = 0; e < 4; ++e) st[e].zero();
 #pragma unroll
-    for (int p = 0; p < S / 2; ++p) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            st[e].add_pair(T, p, (w[2 * p] >> (e * 8)) & 0xFFu, (w[2 * p + 1] >> (e * 8)) & 0xFFu);
+    for (int t = 0; t < NT; ++t) {
+        const uint32_t wa = w[3 * t], wb = w[3 * t + 1], wc = w[3 * t + 2];
+        const uint32_t x01 = __byte_perm(wa, wb, 0x5140);   // c_a0 c_b0 c_a1 c_b1
+        const uint32_t x23 = __byte_perm(wa, wb, 0x7362);   // c_a2 c_b2 c_a3 c_b3
+        const uint32_t k = T.tk[t], kab = T.tab[t];
+        const uint32_t d0 = __dp2a_lo(k, x01, __byte_perm(wc, 0, 0x4440) * kab);
+        const uint32_t d1 = __dp2a_hi(k, x01, __byte_perm(wc, 0, 0x4441) * kab);
+        const uint32_t d2 = __dp2a_lo(k, x23, __byte_perm(wc, 0, 0x4442) * kab);
+        const uint32_t d3 = __dp2a_hi(k, x23, __byte_perm(wc, 0, 0x4443) * kab);
+        st[0].add(T.TP[t], T.trecip48[t], d0);
+        st[1].add(T.TP[t], T.trecip48[t], d1);
+        st[2].add(T.TP[t], T.trecip48[t], d2);
+        st[3].add(T.TP[t], T.trecip48[t], d3);
     }
-    if (S & 1) {
+    if constexpr (S % 3 == 2) {
+        const uint32_t ma = c_mod[S - 2].m, mb = c_mod[S - 1].m;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) st[e].add(T, S - 1, (w[S - 1] >> (e * 8)) & 0xFFu);
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t d = ((w[S - 2] >> (8 * e)) & 0xFFu) * mb + ((w[S - 1] >> (8 * e)) & 0xFFu) * ma;
+            st[e].add(T.DP, T.drecip48, d);
+        }
+    } else if constexpr (S % 3 == 1) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) st[e].add(T, S - 1, (w[S - 1] >> (8 * e)) & 0xFFu);
     }
     const int sa = sA[i];
     double* crow = C + i * N;
@@ -1115,7 +1147,7 @@ __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef,
 }
 
 template <int S>
-__global__ void __launch_bounds__(256) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
+__global__ void __launch_bounds__(128) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
                                                   long long M, long long N, const int32_t* __restrict__ sA,
                                                   const int32_t* __restrict__ sB, double* __restrict__ C) {
     const long long chunks = (N + 3) >> 2;
@@ -1152,27 +1184,80 @@ __global__ void __launch_bounds__(256) k_reconstruct2(const int32_t* __restrict_
 // Scheme I: C = sum over g = 2..S+1 (in that order) of double(C_g) * scale_g,
 // each update one fused multiply-add from +0.0, which is the sequence of the
 // reference's per-group launches (step4_reconstruction.hpp:21-49,
-// pipeline.cu:102-135 after the memset at pipeline.cu:72).
+// pipeline.cu:102-135 after the memset at pipeline.cu:72).  scale_g is
+// ldexp(u_i v_j, 2 beta - beta g) with u_i v_j an exact power of two (or 0 /
+// inf at the exponent extremes); where u_i v_j is normal and the result stays
+// normal that is the product with the exact power 2^(2 beta - beta g), and
+// ldexp itself is called otherwise.  One thread per 4 consecutive columns of
+// a row: one 16-byte load per group plane (all S issued together, S fixed at
+// compile time), the scale exponents and powers computed once per row and
+// column, 4 results per thread.
+// ldexp for the rare scales that leave the normal range (kept out of line).
+__device__ __noinline__ double ldexp_outlined(double x, int k) { return ldexp(x, k); }
+
+template <int S>
+__device__ __forceinline__ void reconstruct1_chunk(const int32_t* __restrict__ ctc, long long Np, long long N,
+                                                   size_t plane, int beta, const int32_t* __restrict__ negA,
+                                                   const int32_t* __restrict__ negB, double* __restrict__ C,
+                                                   long long chunks, long long id) {
+    constexpr int kBatch = 4;   // group planes loaded together
+    const long long i = id / chunks, j0 = (id - i * chunks) << 2;
+    const int4* src = reinterpret_cast<const int4*>(ctc + (size_t)i * Np + j0);
+    const size_t plane4 = plane >> 2;
+    int4 v[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch && b < S; ++b) v[b] = __ldg(src + b * plane4);
+    const double ui = ldexp(1.0, -negA[i] + 1 - beta);
+    double uv[4];
+    int lim[4];   // smallest scale exponent k with uv * 2^k still normal (INT_MAX: never)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const long long j = j0 + e;
+        uv[e] = __dmul_rn(ui, ldexp(1.0, (j < N ? -negB[j] : 0) + 1 - beta));
+        const int E = (int)((unsigned long long)__double_as_longlong(uv[e]) >> 52) & 0x7FF;
+        lim[e] = (E == 0 || E == 0x7FF) ? 0x7FFFFFFF : -1022 - (E - 1023);
+    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int g0 = 0; g0 < S; g0 += kBatch) {
+        int4 nv[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b)
+            if (g0 + kBatch + b < S) nv[b] = __ldg(src + (g0 + kBatch + b) * plane4);
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const int g = g0 + b;
+            if (g >= S) break;
+            const int k = -beta * g;   // 2 beta - beta (g + 2): plane g holds group g + 2
+            const double p = __longlong_as_double((long long)(k + 1023) << 52);   // k in [-1022, 0]
+            const int val[4] = {v[b].x, v[b].y, v[b].z, v[b].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double scale = k >= lim[e] ? __dmul_rn(uv[e], p) : ldexp_outlined(uv[e], k);
+                acc[e] = __fma_rn((double)val[e], scale, acc[e]);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b)
+            if (g0 + kBatch + b < S) v[b] = nv[b];
+    }
+    double* crow = C + i * N;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+        if (j0 + e < N) crow[j0 + e] = acc[e];
+}
+
+template <int S>
 __global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict__ ctc, long long Mp, long long Np,
-                                                      long long M, long long N, int S, int beta,
+                                                      long long M, long long N, int beta,
                                                       const int32_t* __restrict__ negA,
                                                       const int32_t* __restrict__ negB, double* __restrict__ C) {
-    const long long total = M * N;
+    const long long chunks = (N + 3) >> 2;
+    const long long total = M * chunks;
     const size_t plane = (size_t)Mp * (size_t)Np;
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x) {
-        const long long i = id / N, j = id - i * N;
-        const double ui = ldexp(1.0, -negA[i] + 1 - beta);
-        const double vj = ldexp(1.0, -negB[j] + 1 - beta);
-        const double uv = __dmul_rn(ui, vj);
-        const int32_t* src = ctc + (size_t)i * Np + j;
-        double acc = 0.0;
-        for (int g = 2; g <= S + 1; ++g) {
-            const double scale = ldexp(uv, -beta * g + 2 * beta);
-            acc = __fma_rn((double)__ldg(src + (size_t)(g - 2) * plane), scale, acc);
-        }
-        C[id] = acc;
-    }
+         id += (long long)gridDim.x * blockDim.x)
+        reconstruct1_chunk<S>(ctc, Np, N, plane, beta, negA, negB, C, chunks, id);
 }
 
 // ---------------------------------------------------------------------------
@@ -1500,11 +1585,11 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
                             const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st) {
     long long total = (long long)M * (long long)((N + 3) / 4);
     if (total == 0) return cudaSuccess;
-    const int grid = grid_for(total, 256, sms, 16);
+    const int grid = grid_for(total, 128, sms, 32);
     const long long MP = (long long)Mp, NP = (long long)Np, MM = (long long)M, NN = (long long)N;
     switch (S) {
 #define OZA_CASE(n) \
-    case n: k_crt_coef<n><<<grid, 256, 0, st>>>(coef, MP, NP, MM, NN, shiftA, shiftB, C); break;
+    case n: k_crt_coef<n><<<grid, 128, 0, st>>>(coef, MP, NP, MM, NN, shiftA, shiftB, C); break;
         OZA_FOR_EACH_S(OZA_CASE)
 #undef OZA_CASE
         default: return cudaErrorInvalidValue;
@@ -1513,14 +1598,19 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
 }
 
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
-                                const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st) {
-    long long total = (long long)M * (long long)N;
+                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st) {
+    const long long total = (long long)M * (long long)((N + 3) / 4);
     if (total == 0) return cudaSuccess;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int grid = grid_for(total, 256, sms, 16);
-    k_reconstruct1<<<grid, 256, 0, st>>>(ctc, Mp, Np, M, N, S, beta, negA, negB, C);
+    if (Np % 4 != 0 || beta < 1 || beta * S > 1022) return cudaErrorInvalidValue;
+    const int grid = grid_for(total, 256, sms, 16);
+    const long long MP = (long long)Mp, NP = (long long)Np, MM = (long long)M, NN = (long long)N;
+    switch (S) {
+#define OZA_CASE(n) \
+    case n: k_reconstruct1<n><<<grid, 256, 0, st>>>(ctc, MP, NP, MM, NN, beta, negA, negB, C); break;
+        OZA_FOR_EACH_S(OZA_CASE)
+#undef OZA_CASE
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -79,7 +79,7 @@ cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t
 cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M, size_t N, int S,
                             const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st);
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
-                                const int32_t* negA, const int32_t* negB, double* C, cudaStream_t st);
+                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st);
 
 // Grouped Scheme II: many independent GEMMs, each stage one launch (the
 // slicers and the CRT one per slice-count class).  Buffers as in a Scheme II

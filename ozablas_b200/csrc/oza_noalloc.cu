@@ -185,7 +185,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
         NA_TRY(oza::launch_crt_coef(out, Mp, Np, M, N, slices, shiftA, shiftB, C, sms, st), "step 4");
     else
         NA_TRY(oza::launch_reconstruct1(reinterpret_cast<int32_t*>(out), Mp, Np, M, N, slices, beta, shiftA, shiftB,
-                                        C, st),
+                                        C, sms, st),
                "step 4");
 #undef NA_TRY
     return OZA_OK;
