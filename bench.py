@@ -572,6 +572,13 @@ def run_precision_suite(args, local):
         target = oz.block_error(ex, dA, dB, dD, M, N, K, block, tune_seed)
         dgemm_val = oz.block_error(ex, dA, dB, dD, M, N, K, block, val_seed)
         flops = 2.0 * M * N * K
+        # the accuracy knob's own choice of scheme and count for this target
+        t0 = time.perf_counter()
+        try:
+            chosen = oz.autotune_scheme(ex, dA, dB, M, N, K, target, block, tune_seed)[:2]
+        except oz.OzaError:
+            chosen = (None, None)
+        choose_s = time.perf_counter() - t0
         for scheme in (2, 1):
             t0 = time.perf_counter()
             try:
@@ -607,6 +614,9 @@ def run_precision_suite(args, local):
                            "zero_mask": "Bernoulli(0.05), MT19937 seed 1234",
                            "input_seed": 42},
                 "slices": S, "target_met_on_tuning_block": met,
+                "chosen_by_knob": chosen == (scheme, S), "knob_choice": {"scheme": chosen[0], "slices": chosen[1],
+                                                                         "autotune_scheme_s": choose_s},
+                "validation_meets_dgemm": bool(val <= dgemm_val),
                 "target_rel_err": target, "tuned_block_err": tuned,
                 "validation_err": val, "cublas_dgemm_validation_err": dgemm_val,
                 "scaled_entries_err": scaled, "cublas_dgemm_scaled_entries_err": scaled_d,
@@ -832,8 +842,9 @@ def ref_workspace_bytes(M, N, K, S):
 def serve_requests(n, seed=99):
     """M, N, K log-uniform in [128, 8192] (K capped so the reference's workspace
     formula 4(M+N) + S(MK+KN) + 4S MN is at most 2 GB), phi in {0.5, 2}, target
-    in {1e-12, 1e-15} -> slice count from the calibrated table (20 where it is
-    not reached)."""
+    in {1e-12, 1e-15} -> scheme and slice count from the calibrated tables
+    (oza_scheme_for_target: Scheme II where its moduli reach the target, else
+    Scheme I; 20 where neither table reaches it)."""
     import numpy as np
     import ozablas_b200 as oz
     rng = np.random.default_rng(seed)
@@ -842,11 +853,12 @@ def serve_requests(n, seed=99):
         M, N, K = (int(v) for v in np.rint(np.exp(rng.uniform(math.log(128), math.log(8192), 3))))
         phi = float(rng.choice([0.5, 2.0]))
         target = float(rng.choice([1e-12, 1e-15]))
-        S = oz.slices_for_target(target, K, phi)
+        sc, S = oz.scheme_for_target(target, K, phi)
         while ref_workspace_bytes(M, N, K, min(S, 20)) > SERVE_WS_CAP and K > 128:
             K = max(128, K * 3 // 4)
-            S = oz.slices_for_target(target, K, phi)
-        out.append(dict(M=M, N=N, K=K, phi=phi, target=target, S=min(S, 20), table_reaches_target=S <= 20))
+            sc, S = oz.scheme_for_target(target, K, phi)
+        out.append(dict(M=M, N=N, K=K, phi=phi, target=target, scheme=sc, S=min(S, 20),
+                        table_reaches_target=S <= 20))
     return out
 
 
@@ -882,6 +894,13 @@ def run_serve_suite(args, local):
         C.append(torch.empty(r["M"], r["N"], dtype=torch.float64, device=dev))
     torch.cuda.synchronize()
     flops = [2.0 * r["M"] * r["N"] * r["K"] for r in reqs]
+
+    def _ws(r):
+        cls = oz.WorkspaceScheme2 if r["scheme"] == 2 else oz.WorkspaceScheme1
+        return cls(ex, r["M"], r["N"], r["K"], r["S"])
+
+    def _gemm(r):
+        return oz.ozaki_scheme2_gemm if r["scheme"] == 2 else oz.ozaki_scheme1_gemm
     total_flops = sum(flops)
 
     def served(arrivals):
@@ -895,7 +914,7 @@ def run_serve_suite(args, local):
                 dt = arrivals[i] - (time.perf_counter() - t0)
                 if dt > 0:
                     time.sleep(dt)
-                ids[i] = srv.submit(A[i], B[i], C[i], r["S"])
+                ids[i] = srv.submit(A[i], B[i], C[i], r["S"], scheme=r["scheme"])
             st = [srv.wait(i, timeout=600) for i in ids]
             sst = srv.stats()
         finally:
@@ -909,10 +928,10 @@ def run_serve_suite(args, local):
         beforehand, second call timed with events)."""
         out = []
         for i, r in enumerate(reqs):
-            ws = oz.WorkspaceScheme2(ex, r["M"], r["N"], r["K"], r["S"])
-            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i])
+            ws = _ws(r)
+            _gemm(r)(ws, A[i], B[i], C[i])
             t = oz.OzaTimings()
-            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i], t)
+            _gemm(r)(ws, A[i], B[i], C[i], t)
             out.append(t.total_ms * 1e-3)
             del ws
         return out
@@ -933,8 +952,8 @@ def run_serve_suite(args, local):
             now = time.perf_counter() - t0
             if arrivals[i] > now:
                 time.sleep(arrivals[i] - now)
-            ws = oz.WorkspaceScheme2(ex, r["M"], r["N"], r["K"], r["S"])
-            oz.ozaki_scheme2_gemm(ws, A[i], B[i], C[i])
+            ws = _ws(r)
+            _gemm(r)(ws, A[i], B[i], C[i])
             ex.synchronize()
             del ws
             lat.append(time.perf_counter() - t0 - arrivals[i])
@@ -957,8 +976,8 @@ def run_serve_suite(args, local):
     for i in rng.choice(len(reqs), 16, replace=False):
         r = reqs[i]
         e = oz.block_error(ex, A[i], B[i], C[i], r["M"], r["N"], r["K"], 128, 3)
-        acc.append({"target": r["target"], "slices": r["S"], "err": e, "met": e <= r["target"],
-                    "table_reaches_target": r["table_reaches_target"]})
+        acc.append({"target": r["target"], "scheme": r["scheme"], "slices": r["S"], "err": e,
+                    "met": e <= r["target"], "table_reaches_target": r["table_reaches_target"]})
 
     def pct(x, q):
         return float(np.percentile(np.asarray(x) * 1e3, q))
@@ -968,7 +987,9 @@ def run_serve_suite(args, local):
         "config": {"workload": f"served_dgemm_stream_{len(reqs)}_requests",
                    "dims": "M, N, K log-uniform in [128, 8192], K capped so 4(M+N)+S(MK+KN)+4S*MN <= 2 GB",
                    "phi": [0.5, 2.0], "targets": [1e-12, 1e-15],
-                   "slices": "oza_slices_for_target (20 where the table does not reach the target)",
+                   "slices": "oza_scheme_for_target: scheme and count from the calibrated tables (20 where "
+                             "neither reaches the target)",
+                   "scheme_i_requests": sum(1 for r in reqs if r["scheme"] == 1),
                    "budget_bytes": SERVE_BUDGET, "max_inflight": 2, "max_batch": 64,
                    "total_gflop": total_flops / 1e9, "request_seed": 99},
     }

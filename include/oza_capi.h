@@ -55,13 +55,27 @@ typedef struct oza_timings {
 /* Workspace flags. */
 #define OZA_WS_MATERIALIZE 0x1u  /* keep every intermediate (slices, INT32 products) in
                                     the workspace buffers, for inspection and parity */
+#define OZA_WS_REFERENCE_LAYOUT 0x2u  /* implies MATERIALIZE; after each GEMM also copy the
+                                    intermediates into buffers laid out as the reference's
+                                    workspace getters return them (see OZA_BUF_*), which
+                                    oza_ws_get_ptr then returns; for inspection and for code
+                                    that reads the reference's buffers (costs a copy per call) */
 
-/* Buffers exposed by oza_ws_get_ptr (reference getters workspace.hpp:174-178). */
+/* Buffers exposed by oza_ws_get_ptr (reference getters workspace.hpp:174-178).
+ * Default layouts (those the sm_100a kernels use), and with
+ * OZA_WS_REFERENCE_LAYOUT the reference's own (workspace.cpp:21-126,
+ * pipeline.cu:40-265):                                 reference layout:
+ *   OZA_BUF_A_SLICES  int8 [S][Mp][Kp] K-major, padded  int8 [S][M][K]
+ *   OZA_BUF_B_SLICES  int8 [S][Np][Kp] (B transposed)   int8 [S][K][N]
+ *   OZA_BUF_C_TC      int32[G][Mp][Np] (MATERIALIZE)    Scheme II: int32 [S][M][N];
+ *                                                       Scheme I: int32 [M][N], the
+ *                                                       last group (g = S + 1), as the
+ *                                                       reference's buffer holds it */
 #define OZA_BUF_SHIFT_A  0  /* int32[M]                                      */
 #define OZA_BUF_SHIFT_B  1  /* int32[N]                                      */
-#define OZA_BUF_A_SLICES 2  /* int8 [S][Mp][Kp]   (K-major, zero padded)     */
-#define OZA_BUF_B_SLICES 3  /* int8 [S][Np][Kp]   (K-major: B transposed)    */
-#define OZA_BUF_C_TC     4  /* int32[G][Mp][Np]   (only with MATERIALIZE)    */
+#define OZA_BUF_A_SLICES 2
+#define OZA_BUF_B_SLICES 3
+#define OZA_BUF_C_TC     4
 
 /* Workspace geometry (padded extents of the buffers above). */
 typedef struct oza_ws_info {
@@ -238,13 +252,14 @@ oza_status_t oza_group_get_info(oza_group_t g, oza_group_info_t* info);
 oza_status_t oza_group_device_error(oza_group_t g, int* code);
 
 /* ---- request loop ---------------------------------------------------------- */
-/* A server for streams of independent Scheme II FP64 GEMMs with continuous
+/* A server for streams of independent FP64 GEMMs with continuous
  * batching.  Requests are admitted in arrival order while their workspaces fit
  * in a device arena of `workspace_budget` bytes (allocated at creation) and one
- * of `max_inflight` stream slots is free; everything admitted together runs as
- * one grouped batch (the oza_group kernels).  Batches on different slots
- * overlap on the device.  Each result is bit-identical to oza_gemm on the same
- * request alone.  Extension: the reference has no request loop. */
+ * of `max_inflight` stream slots is free; the Scheme II requests admitted
+ * together run as one grouped batch (the oza_group kernels), a Scheme I
+ * request as a batch of its own.  Batches on different slots overlap on the
+ * device.  Each result is bit-identical to oza_gemm on the same request alone.
+ * Extension: the reference has no request loop. */
 typedef struct oza_server* oza_server_t;
 
 typedef struct {
@@ -271,15 +286,18 @@ oza_status_t oza_server_create(oza_exec_t ex, const oza_server_config_t* cfg, oz
 /* Runs every queued request to completion, then frees the server. */
 oza_status_t oza_server_destroy(oza_server_t s);
 /* Queue C = A * B (row-major device buffers, valid until the request
- * completes).  OZA_OOM if the request alone exceeds the budget. */
-oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, const double* A, const double* B,
-                               double* C, int slices, uint64_t* id);
+ * completes) by `scheme` (OZA_SCHEME2: batched with other Scheme II requests;
+ * OZA_SCHEME1: run as a batch of its own) with `slices` slices/moduli, e.g.
+ * as oza_scheme_for_target chooses them.  OZA_OOM if the request alone
+ * exceeds the budget. */
+oza_status_t oza_server_submit(oza_server_t s, int scheme, size_t M, size_t N, size_t K, const double* A,
+                               const double* B, double* C, int slices, uint64_t* id);
 /* Wait for a request (timeout_s < 0: no limit; OZA_TIMEOUT if it expires) and
  * release its record; stats (optional) receives its timestamps. */
 oza_status_t oza_server_wait(oza_server_t s, uint64_t id, double timeout_s, oza_request_stats_t* stats);
 oza_status_t oza_server_get_stats(oza_server_t s, oza_server_stats_t* out);
 /* Workspace bytes one request takes from the arena (0 for invalid sizes). */
-size_t oza_server_request_bytes(size_t M, size_t N, size_t K, int slices);
+size_t oza_server_request_bytes(int scheme, size_t M, size_t N, size_t K, int slices);
 
 /* ---- accuracy tools ------------------------------------------------------- */
 /* Maximum relative error of C (M x N, device) against a double-double
@@ -300,6 +318,17 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
                                  const double* B, double target_rel_err, int block, unsigned seed, int* slices,
                                  double* achieved_err);
 
+/* The accuracy knob's choice of scheme as well: Scheme II (S INT8 GEMMs for
+ * S moduli) or Scheme I (S (S + 1) / 2 GEMMs for S slices), whichever meets
+ * `target_rel_err` on the seeded block sample with fewer INT8 GEMMs --
+ * Scheme I where Scheme II's 20 moduli miss the target (wide exponent ranges,
+ * deep K) or where K exceeds Scheme II's INT32-exact bound.  Returns
+ * OZA_UNSUPPORTED, with the scheme whose 20-slice error is lower, if neither
+ * reaches it.  Extension: the reference leaves scheme and slices to the caller. */
+oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                                 double target_rel_err, int block, unsigned seed, int* scheme, int* slices,
+                                 double* achieved_err);
+
 /* Slice count for a maximum-relative-error target without running anything:
  * a table measured on B200 (ozablas_b200/calibrate_slices.py) for K = 128 ..
  * 65536 and inputs (U - 0.5) * exp(phi * N(0,1)), phi = 0.5 .. 4, errors over
@@ -308,6 +337,13 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
  * not reach the target at the calibrated points, 0 for invalid arguments.
  * Extension: the reference leaves `slices` to the caller. */
 int oza_slices_for_target(double target_rel_err, size_t K, double phi);
+/* Scheme and slice count for a target without running anything, from the same
+ * calibration for both schemes: returns OZA_SCHEME2 or OZA_SCHEME1 (the one
+ * reaching the target with fewer INT8 GEMMs; Scheme II on a tie), *slices its
+ * count; Scheme I with *slices = 21 if neither reaches the target with 20.
+ * 0 for invalid arguments.  Extension: the reference leaves the choice to the
+ * caller. */
+int oza_scheme_for_target(double target_rel_err, size_t K, double phi, int* slices);
 
 /* ---- host utilities ------------------------------------------------------- */
 /* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from

@@ -1,12 +1,16 @@
 // <ozablas/core/workspace.hpp> -- drop-in workspaces and OzaTimings.
 // Mirrors include/ozablas/core/workspace.hpp:14-103 of IlyaNyrkov/ozablas.
 //
-// Layout note: the device buffers are laid out for the sm_100a kernels, not
-// as in the reference.  Slices/residues are K-major and zero padded:
-// get_A_slices() is int8 [S][Mp][Kp], get_B_slices() is int8 [S][Np][Kp]
-// (B transposed), get_C_tc() is int32 [S][Mp][Np] with plane g holding
-// group g (Scheme II: residue g; Scheme I: slice-sum group g+2).  The padded
-// extents are get_Mp()/get_Np()/get_Kp().
+// Layout note: by default the device buffers are laid out for the sm_100a
+// kernels, not as in the reference.  Slices/residues are K-major and zero
+// padded: get_A_slices() is int8 [S][Mp][Kp], get_B_slices() is int8
+// [S][Np][Kp] (B transposed), get_C_tc() is int32 [S][Mp][Np] with plane g
+// holding group g (Scheme II: residue g; Scheme I: slice-sum group g+2), and
+// null for Scheme II, whose INT32 products never reach memory.  The padded
+// extents are get_Mp()/get_Np()/get_Kp().  Constructed with
+// WorkspaceLayout::Reference, the getters return the reference's own layouts
+// instead, refreshed by every GEMM call: A slices [S][M][K], B slices
+// [S][K][N], C_tc [S][M][N] (Scheme II) or the last group [M][N] (Scheme I).
 #pragma once
 
 #include <cstddef>
@@ -19,11 +23,19 @@ struct oza_workspace;
 
 namespace ozablas {
 
+/** Layout of the intermediates the workspace getters expose (extension). */
+enum class WorkspaceLayout {
+    Device,      ///< the sm_100a kernels' padded K-major planes (default)
+    Reference,   ///< also kept in the reference's layouts, returned by the getters
+};
+
 class WorkspaceScheme1 {
 public:
     /** Throws std::invalid_argument (null executor, slices < 1), std::bad_alloc,
      *  std::runtime_error (executor is not a CudaExecutor or CUDA failure). */
     WorkspaceScheme1(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices);
+    WorkspaceScheme1(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices,
+                     WorkspaceLayout layout);
     ~WorkspaceScheme1();
     WorkspaceScheme1(const WorkspaceScheme1&) = delete;
     WorkspaceScheme1& operator=(const WorkspaceScheme1&) = delete;
@@ -55,6 +67,8 @@ public:
     /** Throws std::invalid_argument (null executor, slices outside 1..20),
      *  std::bad_alloc, std::runtime_error. */
     WorkspaceScheme2(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices);
+    WorkspaceScheme2(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices,
+                     WorkspaceLayout layout);
     ~WorkspaceScheme2();
     WorkspaceScheme2(const WorkspaceScheme2&) = delete;
     WorkspaceScheme2& operator=(const WorkspaceScheme2&) = delete;

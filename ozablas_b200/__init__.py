@@ -26,7 +26,8 @@ __all__ = [
     "LIB_PATH", "OzaError", "OzaTimeoutError", "OzaTimings", "CudaExecutor", "CpuExecutor",
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
-    "autotune_slices", "GroupGemm", "Server", "slices_for_target", "ozaki_gemm_host", "selftest_wait_timeout",
+    "autotune_slices", "autotune_scheme", "GroupGemm", "Server", "slices_for_target", "scheme_for_target",
+    "ozaki_gemm_host", "selftest_wait_timeout",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -36,6 +37,7 @@ HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "oza_capi.h")
 OZA_OK, OZA_INVALID_ARG, OZA_OOM, OZA_CUDA_ERROR, OZA_TIMEOUT, OZA_UNSUPPORTED = range(6)
 OZA_SCHEME1, OZA_SCHEME2 = 1, 2
 OZA_WS_MATERIALIZE = 0x1
+OZA_WS_REFERENCE_LAYOUT = 0x2
 OZA_GROUP_NO_GRAPH = 0x2
 BUF_SHIFT_A, BUF_SHIFT_B, BUF_A_SLICES, BUF_B_SLICES, BUF_C_TC = range(5)
 
@@ -148,11 +150,14 @@ def lib() -> ctypes.CDLL:
         "oza_group_device_error": (I, [P, ctypes.POINTER(I)]),
         "oza_server_create": (I, [P, ctypes.POINTER(_ServerConfig), ctypes.POINTER(P)]),
         "oza_server_destroy": (I, [P]),
-        "oza_server_submit": (I, [P, S, S, S, P, P, P, I, ctypes.POINTER(ctypes.c_uint64)]),
+        "oza_server_submit": (I, [P, I, S, S, S, P, P, P, I, ctypes.POINTER(ctypes.c_uint64)]),
         "oza_server_wait": (I, [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_RequestStats)]),
         "oza_server_get_stats": (I, [P, ctypes.POINTER(_ServerStats)]),
-        "oza_server_request_bytes": (S, [S, S, S, I]),
+        "oza_server_request_bytes": (S, [I, S, S, S, I]),
         "oza_slices_for_target": (I, [ctypes.c_double, S, ctypes.c_double]),
+        "oza_scheme_for_target": (I, [ctypes.c_double, S, ctypes.c_double, ctypes.POINTER(I)]),
+        "oza_autotune_scheme": (I, [P, S, S, S, P, P, ctypes.c_double, I, U, ctypes.POINTER(I), ctypes.POINTER(I),
+                                    ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -252,14 +257,15 @@ class CudaExecutor:
 class _Workspace:
     _scheme = 0
 
-    def __init__(self, executor, M: int, N: int, K: int, slices: int, materialize: bool = False):
+    def __init__(self, executor, M: int, N: int, K: int, slices: int, materialize: bool = False,
+                 reference_layout: bool = False):
         if executor is None:
             raise ValueError("OzaBLAS: Executor cannot be null.")
         if not isinstance(executor, CudaExecutor):
             raise OzaError("OzaBLAS: No suitable hardware backend found for the provided Executor.")
         self._exec = executor   # keeps the executor alive, like the reference's shared_ptr
         h = ctypes.c_void_p()
-        flags = OZA_WS_MATERIALIZE if materialize else 0
+        flags = (OZA_WS_MATERIALIZE if materialize else 0) | (OZA_WS_REFERENCE_LAYOUT if reference_layout else 0)
         _check(lib().oza_ws_create(executor.handle, self._scheme, int(M), int(N), int(K), int(slices),
                                    flags, ctypes.byref(h)))
         self._h = h
@@ -441,11 +447,11 @@ class GroupGemm:
 
 
 class Server:
-    """Request loop with continuous batching for Scheme II FP64 GEMMs
-    (extension; the reference has no request loop).  Requests are admitted in
-    arrival order while their workspaces fit in `workspace_budget` bytes of
-    device memory and one of `max_inflight` stream slots is free; each batch
-    runs the grouped kernels.
+    """Request loop with continuous batching for FP64 GEMMs (extension; the
+    reference has no request loop).  Requests are admitted in arrival order
+    while their workspaces fit in `workspace_budget` bytes of device memory and
+    one of `max_inflight` stream slots is free; the Scheme II requests of a
+    batch run the grouped kernels, a Scheme I request runs on its own.
 
         srv = Server(ex, 8 << 30)
         rid = srv.submit(A, B, C, slices=16)   # device matrices, kept alive by the caller
@@ -462,18 +468,20 @@ class Server:
         self._h = h
 
     @staticmethod
-    def request_bytes(M: int, N: int, K: int, slices: int) -> int:
-        return int(lib().oza_server_request_bytes(int(M), int(N), int(K), int(slices)))
+    def request_bytes(M: int, N: int, K: int, slices: int, scheme: int = OZA_SCHEME2) -> int:
+        return int(lib().oza_server_request_bytes(int(scheme), int(M), int(N), int(K), int(slices)))
 
     def submit(self, A, B, C, slices: int, M: int | None = None, N: int | None = None,
-               K: int | None = None) -> int:
+               K: int | None = None, scheme: int = OZA_SCHEME2) -> int:
+        """Queue C = A * B with `slices` slices/moduli of `scheme` (Scheme II
+        requests are batched together; a Scheme I request runs on its own)."""
         if M is None:
             M, K = A.shape
             N = B.shape[1]
             if tuple(B.shape) != (K, N) or tuple(C.shape) != (M, N):
                 raise ValueError("shapes do not agree")
         rid = ctypes.c_uint64()
-        _check(lib().oza_server_submit(self._h, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
+        _check(lib().oza_server_submit(self._h, int(scheme), int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
                                        ctypes.c_void_p(_ptr(B)), ctypes.c_void_p(_ptr(C)), int(slices),
                                        ctypes.byref(rid)))
         return rid.value
@@ -579,6 +587,30 @@ def autotune_slices(executor, scheme: int, A, B, M: int, N: int, K: int, target_
                                      ctypes.c_void_p(_ptr(A)), ctypes.c_void_p(_ptr(B)), float(target_rel_err),
                                      int(block), int(seed), ctypes.byref(s), ctypes.byref(e)))
     return s.value, e.value
+
+
+def autotune_scheme(executor, A, B, M: int, N: int, K: int, target_rel_err: float, block: int = 96,
+                    seed: int = 7):
+    """Scheme and slice count meeting target_rel_err on a sampled block with the
+    fewest INT8 GEMMs (Scheme I where Scheme II's 20 moduli miss it); returns
+    (scheme, slices, sampled error).  Raises OzaError if neither scheme reaches it."""
+    sc, s = ctypes.c_int(), ctypes.c_int()
+    e = ctypes.c_double()
+    _check(lib().oza_autotune_scheme(executor.handle, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
+                                     ctypes.c_void_p(_ptr(B)), float(target_rel_err), int(block), int(seed),
+                                     ctypes.byref(sc), ctypes.byref(s), ctypes.byref(e)))
+    return sc.value, s.value, e.value
+
+
+def scheme_for_target(target_rel_err: float, K: int, phi: float = 2.0):
+    """(scheme, slices) for a maximum-relative-error target from the calibrated
+    tables (no GPU work): the scheme reaching it with fewer INT8 GEMMs; slices
+    21 means neither reaches it with 20."""
+    s = ctypes.c_int()
+    sc = int(lib().oza_scheme_for_target(float(target_rel_err), int(K), float(phi), ctypes.byref(s)))
+    if sc == 0:
+        raise ValueError("target must be > 0, K >= 1, phi >= 0")
+    return sc, s.value
 
 
 def slices_for_target(target_rel_err: float, K: int, phi: float = 2.0) -> int:

@@ -91,6 +91,10 @@ struct oza_workspace {
     int8_t* bplanes = nullptr;
     int32_t* ctc = nullptr;          // INT32 group planes (materialised / Scheme I)
     uint8_t* coef = nullptr;         // Scheme II CRT coefficient bytes [S][Mp][Np]
+    // OZA_WS_REFERENCE_LAYOUT: the intermediates in the reference's layouts
+    int8_t* a_ref = nullptr;         // [S][M][K]
+    int8_t* b_ref = nullptr;         // [S][K][N]
+    int32_t* c_ref = nullptr;        // Scheme II [S][M][N]; Scheme I [M][N] (last group)
     bool fused = false;
     int* err = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -127,7 +131,7 @@ void ws_release(oza_workspace* ws) {
     if (h.cin) cudaStreamSynchronize(h.cin);
     if (h.cout) cudaStreamSynchronize(h.cout);
     void* bufs[] = {ws->shiftA, ws->shiftB, ws->colmax, ws->aplanes, ws->bplanes, ws->ctc, ws->coef, ws->err,
-                    h.dA, h.dB, h.dC};
+                    ws->a_ref, ws->b_ref, ws->c_ref, h.dA, h.dB, h.dC};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (auto& e : ws->ev)
@@ -383,7 +387,9 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     if (!out) return fail(OZA_INVALID_ARG, "oza_ws_create: null output handle");
     *out = nullptr;
     if (!ex) return fail(OZA_INVALID_ARG, "OzaBLAS: Executor cannot be null.");
-    if (flags & ~OZA_WS_MATERIALIZE) return fail(OZA_INVALID_ARG, "oza_ws_create: unknown flags 0x%x", flags);
+    if (flags & ~(OZA_WS_MATERIALIZE | OZA_WS_REFERENCE_LAYOUT))
+        return fail(OZA_INVALID_ARG, "oza_ws_create: unknown flags 0x%x", flags);
+    if (flags & OZA_WS_REFERENCE_LAYOUT) flags |= OZA_WS_MATERIALIZE;
     {
         const oza_status_t chk = oza::check_problem("oza_ws_create", scheme, M, N, K, slices);
         if (chk != OZA_OK) return chk;
@@ -418,6 +424,9 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     ws->fused = (scheme == OZA_SCHEME2) && !(flags & OZA_WS_MATERIALIZE);
     const size_t ctc_bytes = ws->fused ? 0 : (size_t)ws->groups * ws->Mp * ws->Np * sizeof(int32_t) + 16;
     const size_t coef_bytes = ws->fused ? (size_t)slices * ws->Mp * ws->Np + 16 : 0;
+    const bool ref_layout = (flags & OZA_WS_REFERENCE_LAYOUT) != 0;
+    const size_t S_ = (size_t)slices;
+    const size_t ref_c_planes = scheme == OZA_SCHEME2 ? S_ : 1;
     struct Req {
         void** p;
         size_t bytes;
@@ -430,6 +439,9 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
         {(void**)&ws->ctc, ctc_bytes},
         {(void**)&ws->coef, coef_bytes},
         {(void**)&ws->err, sizeof(int)},
+        {(void**)&ws->a_ref, ref_layout ? S_ * M * K + 16 : 0},
+        {(void**)&ws->b_ref, ref_layout ? S_ * K * N + 16 : 0},
+        {(void**)&ws->c_ref, ref_layout ? ref_c_planes * M * N * sizeof(int32_t) + 16 : 0},
     };
     for (auto& r : reqs) {
         if (r.bytes == 0) continue;
@@ -467,9 +479,9 @@ oza_status_t oza_ws_get_ptr(oza_ws_t ws, int which, void** ptr) {
     switch (which) {
         case OZA_BUF_SHIFT_A: *ptr = ws->shiftA; break;
         case OZA_BUF_SHIFT_B: *ptr = ws->shiftB; break;
-        case OZA_BUF_A_SLICES: *ptr = ws->aplanes; break;
-        case OZA_BUF_B_SLICES: *ptr = ws->bplanes; break;
-        case OZA_BUF_C_TC: *ptr = ws->ctc; break;
+        case OZA_BUF_A_SLICES: *ptr = ws->a_ref ? (void*)ws->a_ref : (void*)ws->aplanes; break;
+        case OZA_BUF_B_SLICES: *ptr = ws->b_ref ? (void*)ws->b_ref : (void*)ws->bplanes; break;
+        case OZA_BUF_C_TC: *ptr = ws->c_ref ? (void*)ws->c_ref : (void*)ws->ctc; break;
         default: return fail(OZA_INVALID_ARG, "oza_ws_get_ptr: unknown buffer %d", which);
     }
     return OZA_OK;
@@ -582,9 +594,19 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
                          "step4 sum");
         }
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[4], st), "CUDA: event record");
+        if (ws->a_ref) {
+            // OZA_WS_REFERENCE_LAYOUT: the reference's buffers, outside the timed steps.
+            const int c_first = ws->scheme == OZA_SCHEME2 ? 0 : ws->groups - 1;
+            const int c_count = ws->scheme == OZA_SCHEME2 ? ws->groups : 1;
+            OZA_CUDA_TRY(oza::launch_to_reference_layout(ws->aplanes, ws->bplanes, ws->ctc, ws->S, ws->groups, M, N,
+                                                         K, ws->Mp, ws->Np, ws->Kp, ws->a_ref, ws->b_ref, ws->c_ref,
+                                                         c_first, c_count, st),
+                         "reference-layout copies");
+        }
     }
     if (timings) {
         OZA_CUDA_TRY(cudaEventSynchronize(ws->ev[4]), "CUDA: event synchronize");
+        if (ws->a_ref) OZA_CUDA_TRY(cudaStreamSynchronize(st), "CUDA: stream synchronize");
         cudaEventElapsedTime(&timings->step1_ms, ws->ev[0], ws->ev[1]);
         cudaEventElapsedTime(&timings->step2_ms, ws->ev[1], ws->ev[2]);
         cudaEventElapsedTime(&timings->step3_ms, ws->ev[2], ws->ev[3]);

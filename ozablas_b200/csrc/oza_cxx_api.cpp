@@ -42,6 +42,10 @@ oza_ws_info_t info_of(oza_workspace* ws) {
     return info;
 }
 
+unsigned layout_flags(WorkspaceLayout layout) {
+    return layout == WorkspaceLayout::Reference ? OZA_WS_REFERENCE_LAYOUT : 0u;
+}
+
 void* buf(oza_workspace* ws, int which) {
     void* p = nullptr;
     check(oza_ws_get_ptr(ws, which, &p));
@@ -94,11 +98,15 @@ HipExecutor::HipExecutor(int) { throw std::runtime_error("OzaBLAS was not compil
 
 // ------------------------------------------------------------- workspaces
 WorkspaceScheme1::WorkspaceScheme1(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices)
+    : WorkspaceScheme1(std::move(exec), M, N, K, slices, WorkspaceLayout::Device) {}
+
+WorkspaceScheme1::WorkspaceScheme1(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices,
+                                   WorkspaceLayout layout)
     : exec_(std::move(exec)), M_(M), N_(N), K_(K), slices_(slices) {
     if (!exec_) throw std::invalid_argument("OzaBLAS: Executor cannot be null.");
     if (slices_ < 1) throw std::invalid_argument("OzaBLAS: Slices must be >= 1.");
     const CudaExecutor& cu = need_cuda(exec_);
-    check(oza_ws_create(cu.native(), OZA_SCHEME1, M, N, K, slices, 0u, &ws_));
+    check(oza_ws_create(cu.native(), OZA_SCHEME1, M, N, K, slices, layout_flags(layout), &ws_));
 }
 WorkspaceScheme1::~WorkspaceScheme1() { oza_ws_destroy(ws_); }
 int32_t* WorkspaceScheme1::get_shift_A() const { return static_cast<int32_t*>(buf(ws_, OZA_BUF_SHIFT_A)); }
@@ -111,11 +119,15 @@ size_t WorkspaceScheme1::get_Np() const { return info_of(ws_).Np; }
 size_t WorkspaceScheme1::get_Kp() const { return info_of(ws_).Kp; }
 
 WorkspaceScheme2::WorkspaceScheme2(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices)
+    : WorkspaceScheme2(std::move(exec), M, N, K, slices, WorkspaceLayout::Device) {}
+
+WorkspaceScheme2::WorkspaceScheme2(std::shared_ptr<const Executor> exec, size_t M, size_t N, size_t K, int slices,
+                                   WorkspaceLayout layout)
     : exec_(std::move(exec)), M_(M), N_(N), K_(K), slices_(slices) {
     if (!exec_) throw std::invalid_argument("OzaBLAS: Executor cannot be null.");
     if (slices_ < 1 || slices_ > 20) throw std::invalid_argument("OzaBLAS: Scheme II supports between 1 and 20 slices.");
     const CudaExecutor& cu = need_cuda(exec_);
-    check(oza_ws_create(cu.native(), OZA_SCHEME2, M, N, K, slices, 0u, &ws_));
+    check(oza_ws_create(cu.native(), OZA_SCHEME2, M, N, K, slices, layout_flags(layout), &ws_));
 }
 WorkspaceScheme2::~WorkspaceScheme2() { oza_ws_destroy(ws_); }
 int32_t* WorkspaceScheme2::get_shift_A() const { return static_cast<int32_t*>(buf(ws_, OZA_BUF_SHIFT_A)); }

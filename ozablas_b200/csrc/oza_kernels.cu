@@ -1373,6 +1373,32 @@ __global__ void __launch_bounds__(256) k_group_crt(const GroupProblemDev* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Reference-layout copies of the intermediates (inspection mode only)
+// ---------------------------------------------------------------------------
+// B^T planes [S][Np][Kp] (K-major) -> the reference's B slices [S][K][N]
+// (row-major, unpadded): 32 x 32 byte tiles through shared memory.
+__global__ void __launch_bounds__(256) k_planes_to_kn(const int8_t* __restrict__ src, long long Np, long long Kp,
+                                                      long long K, long long N, int8_t* __restrict__ dst) {
+    __shared__ int8_t tile[32][33];
+    const long long s = blockIdx.z;
+    const long long n0 = (long long)blockIdx.x * 32, k0 = (long long)blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+    const int8_t* sp = src + (size_t)s * Np * Kp;
+    int8_t* dp = dst + (size_t)s * K * N;
+#pragma unroll
+    for (int r = ty; r < 32; r += 8) {
+        const long long n = n0 + r, k = k0 + tx;
+        tile[r][tx] = (n < N && k < K) ? sp[(size_t)n * Kp + k] : 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = ty; r < 32; r += 8) {
+        const long long k = k0 + r, n = n0 + tx;
+        if (k < K && n < N) dp[(size_t)k * N + n] = tile[tx][r];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Self-test of the bounded waits: thread 0 waits, through the same mbar_wait
 // as the GEMM kernels, for a phase of an mbarrier that nothing arrives on.
 // The wait gives up after limit_ns, raises the abort flag and writes the
@@ -1903,6 +1929,28 @@ cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t c
     return cudaSuccess;
 }
 
+
+cudaError_t launch_to_reference_layout(const int8_t* a_planes, const int8_t* b_planes, const int32_t* ctc, int S,
+                                      int groups, size_t M, size_t N, size_t K, size_t Mp, size_t Np, size_t Kp,
+                                      int8_t* a_ref, int8_t* b_ref, int32_t* c_ref, int c_first, int c_count,
+                                      cudaStream_t st) {
+    if (M == 0 || N == 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < S && K && e == cudaSuccess; ++s)
+        e = cudaMemcpy2DAsync(a_ref + (size_t)s * M * K, K, a_planes + (size_t)s * Mp * Kp, Kp, K, M,
+                              cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    if (K) {
+        const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((K + 31) / 32), (unsigned)S);
+        k_planes_to_kn<<<grid, 256, 0, st>>>(b_planes, (long long)Np, (long long)Kp, (long long)K, (long long)N, b_ref);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (c_first < 0 || c_count < 0 || c_first + c_count > groups) return cudaErrorInvalidValue;
+    for (int g = 0; g < c_count && e == cudaSuccess; ++g)
+        e = cudaMemcpy2DAsync(c_ref + (size_t)g * M * N, N * sizeof(int32_t), ctc + (size_t)(c_first + g) * Mp * Np,
+                              Np * sizeof(int32_t), N * sizeof(int32_t), M, cudaMemcpyDeviceToDevice, st);
+    return e;
+}
 
 cudaError_t launch_wait_probe(int* gerr, unsigned long long limit_ns, int* status, cudaStream_t st) {
     k_wait_probe<<<1, 32, 0, st>>>(gerr, limit_ns, status);

@@ -115,6 +115,14 @@ size_t group_plan_units(const GroupPlan* p);
 size_t group_plan_table_bytes(const GroupPlan* p);
 int group_plan_launches(const GroupPlan* p);   // kernel launches per call
 
+// Copies of the intermediates in the reference's layouts: A slices [S][M][K],
+// B slices [S][K][N] (from the K-major B^T planes) and INT32 groups
+// [c_count][M][N] (groups c_first.. of the [groups][Mp][Np] planes).
+cudaError_t launch_to_reference_layout(const int8_t* a_planes, const int8_t* b_planes, const int32_t* ctc, int S,
+                                      int groups, size_t M, size_t N, size_t K, size_t Mp, size_t Np, size_t Kp,
+                                      int8_t* a_ref, int8_t* b_ref, int32_t* c_ref, int c_first, int c_count,
+                                      cudaStream_t st);
+
 // One bounded wait on an mbarrier that nothing arrives on (self-test of the
 // wait bound): *gerr receives the device error code, *status 1 if it returned early.
 cudaError_t launch_wait_probe(int* gerr, unsigned long long limit_ns, int* status, cudaStream_t st);

@@ -1,12 +1,14 @@
-// oza_server.cpp -- request loop for streams of independent FP64 GEMMs
-// (Scheme II) with continuous batching:
+// oza_server.cpp -- request loop for streams of independent FP64 GEMMs with
+// continuous batching:
 //
 //  * submit() queues a request (device pointers, slice count) and returns an id;
 //  * one scheduler thread admits queued requests in arrival order while their
 //    workspaces fit in a device arena of the configured budget and a stream
 //    slot is free, and launches everything it admitted as one grouped batch
 //    (the grouped kernels of oza_kernels.cu) on that slot's stream -- a batch
-//    of one request runs the single-GEMM launch sequence instead;
+//    of one request runs the single-GEMM launch sequence instead.  Scheme I
+//    requests (chosen where Scheme II's 20 moduli cannot reach an accuracy
+//    target) always run as a batch of one;
 //  * up to max_inflight batches run at once on separate streams, so requests
 //    that arrive while a batch is on the GPU are admitted as soon as a slot and
 //    memory free up, and their work overlaps on the device;
@@ -106,20 +108,23 @@ struct Request {
     const double* B = nullptr;
     double* C = nullptr;
     int S = 0;
+    int scheme = OZA_SCHEME2;
     size_t ws_bytes = 0, ws_off = 0;
     oza_request_stats_t stats{};
     bool done = false;
 };
 
-// Per-request workspace: shiftA, shiftB, A planes, B^T planes, coefficient planes.
+// Per-request workspace: shiftA, shiftB, A planes, B^T planes, and the GEMM's
+// output planes: CRT coefficient bytes (Scheme II) or INT32 groups (Scheme I).
 struct WsLayout {
     size_t Mp, Np, Kp, off[5], bytes;
-    WsLayout(size_t M, size_t N, size_t K, int S) {
+    WsLayout(size_t M, size_t N, size_t K, int S, int scheme = OZA_SCHEME2) {
         Mp = oza::round_up(M, oza::kTileM);
         Np = oza::round_up(N, oza::kTileN);
         Kp = oza::round_up(K, oza::kTileK);
         const size_t s = (size_t)S;
-        const size_t sz[5] = {M * 4, N * 4, s * Mp * Kp, s * Np * Kp, s * Mp * Np};
+        const size_t out = s * Mp * Np * (scheme == OZA_SCHEME1 ? sizeof(int32_t) : 1);
+        const size_t sz[5] = {M * 4, N * 4, s * Mp * Kp, s * Np * Kp, out};
         size_t o = 0;
         for (int i = 0; i < 5; ++i) {
             off[i] = o;
@@ -232,12 +237,15 @@ bool oza_server::launch() {
     std::vector<Request*> batch;
     {
         std::lock_guard<std::mutex> lk(mu);
-        // Arrival order; stop at the first request that does not fit now.
+        // Arrival order; stop at the first request that does not fit now.  A
+        // Scheme I request runs alone: it ends a batch and starts its own.
         while (!queue.empty() && (int)batch.size() < cfg.max_batch) {
             Request* r = queue.front();
+            if (r->scheme == OZA_SCHEME1 && !batch.empty()) break;
             if (!arena.alloc(r->ws_bytes, &r->ws_off)) break;
             queue.pop_front();
             batch.push_back(r);
+            if (r->scheme == OZA_SCHEME1) break;
         }
     }
     if (batch.empty()) return false;
@@ -260,7 +268,7 @@ bool oza_server::launch() {
     size_t cofs = 0;
     for (size_t i = 0; i < batch.size(); ++i) {
         const Request* r = batch[i];
-        const WsLayout L(r->M, r->N, r->K, r->S);
+        const WsLayout L(r->M, r->N, r->K, r->S, r->scheme);
         uint8_t* w = arena_base + r->ws_off;
         oza::GroupProblem& p = probs[i];
         p.A = r->A;
@@ -273,7 +281,7 @@ bool oza_server::launch() {
         p.Np = L.Np;
         p.Kp = L.Kp;
         p.S = r->S;
-        p.k_param = oza_scheme2_k_param(r->S, r->K);
+        p.k_param = r->scheme == OZA_SCHEME2 ? oza_scheme2_k_param(r->S, r->K) : 0;
         p.shiftA = reinterpret_cast<int32_t*>(w + L.off[0]);
         p.shiftB = reinterpret_cast<int32_t*>(w + L.off[1]);
         p.a_planes = reinterpret_cast<int8_t*>(w + L.off[2]);
@@ -329,7 +337,10 @@ bool oza_server::launch() {
     }
     const double t = now();
     if (single) {
+        // The single-GEMM launch sequence of oza_gemm (the steps in order).
         const oza::GroupProblem& p = probs[0];
+        const int scheme = batch[0]->scheme;
+        const int beta = scheme == OZA_SCHEME1 ? oza_scheme1_beta(p.K) : 0;
         oza::GemmPlan g;
         g.a_planes = p.a_planes;
         g.b_planes = p.b_planes;
@@ -337,23 +348,26 @@ bool oza_server::launch() {
         g.Mp = p.Mp;
         g.Np = p.Np;
         g.Kp = p.Kp;
-        g.pairs = oza::make_pairs(OZA_SCHEME2, p.S);
+        g.pairs = oza::make_pairs(scheme, p.S);
         g.err = err;
         g.sms = ex->sms;
-        g.ctc = nullptr;
-        g.coef = p.coef;
+        g.ctc = scheme == OZA_SCHEME1 ? reinterpret_cast<int32_t*>(p.coef) : nullptr;
+        g.coef = scheme == OZA_SCHEME2 ? p.coef : nullptr;
         e = cudaMemsetAsync(err, 0, sizeof(int), sl->st);
         if (e == cudaSuccess) e = oza::launch_stats_rows(p.A, p.M, p.K, p.k_param, p.shiftA, ex->sms, sl->st);
         if (e == cudaSuccess) e = oza::launch_stats_cols(p.B, p.K, p.N, p.colmax, ex->sms, sl->st);
         if (e == cudaSuccess)
-            e = oza::launch_slice_rows(OZA_SCHEME2, p.A, p.M, p.K, p.shiftA, p.S, 0, p.k_param, p.a_planes, p.Mp, p.Kp,
+            e = oza::launch_slice_rows(scheme, p.A, p.M, p.K, p.shiftA, p.S, beta, p.k_param, p.a_planes, p.Mp, p.Kp,
                                        ex->sms, sl->st);
         if (e == cudaSuccess)
-            e = oza::launch_slice_cols(OZA_SCHEME2, p.B, p.K, p.N, p.colmax, p.k_param, p.S, 0, p.shiftB, p.b_planes,
+            e = oza::launch_slice_cols(scheme, p.B, p.K, p.N, p.colmax, p.k_param, p.S, beta, p.shiftB, p.b_planes,
                                        p.Np, p.Kp, sl->st);
         if (e == cudaSuccess) e = oza::launch_gemm_i8(g, sl->st);
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && scheme == OZA_SCHEME2)
             e = oza::launch_crt_coef(p.coef, p.Mp, p.Np, p.M, p.N, p.S, p.shiftA, p.shiftB, p.C, ex->sms, sl->st);
+        if (e == cudaSuccess && scheme == OZA_SCHEME1)
+            e = oza::launch_reconstruct1(g.ctc, p.Mp, p.Np, p.M, p.N, p.S, beta, p.shiftA, p.shiftB, p.C, ex->sms,
+                                         sl->st);
     } else {
         std::memcpy(sl->pinned + kAlign, oza::group_plan_image(plan), sl->tab_bytes);
         void* tab = arena_base + sl->tab_off;
@@ -461,25 +475,27 @@ oza_status_t oza_server_create(oza_exec_t ex, const oza_server_config_t* cfg, oz
     return OZA_OK;
 }
 
-size_t oza_server_request_bytes(size_t M, size_t N, size_t K, int slices) {
+size_t oza_server_request_bytes(int scheme, size_t M, size_t N, size_t K, int slices) {
+    if (scheme != OZA_SCHEME1 && scheme != OZA_SCHEME2) return 0;
     if (M == 0 || N == 0 || K == 0 || slices < 1 || slices > 20) return 0;
-    if ((double)K * 125.0 * 125.0 >= 2147483648.0) return 0;   // beyond Scheme II's INT32-exact bound
-    return WsLayout(M, N, K, slices).bytes;
+    // beyond Scheme II's INT32-exact bound
+    if (scheme == OZA_SCHEME2 && (double)K * 125.0 * 125.0 >= 2147483648.0) return 0;
+    return WsLayout(M, N, K, slices, scheme).bytes;
 }
 
-oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, const double* A, const double* B,
-                               double* C, int slices, uint64_t* id) {
+oza_status_t oza_server_submit(oza_server_t s, int scheme, size_t M, size_t N, size_t K, const double* A,
+                               const double* B, double* C, int slices, uint64_t* id) {
     // Sizes first (the same limits as oza_ws_create), then the handles.
     if (M == 0 || N == 0 || K == 0 || M > (1u << 30) || N > (1u << 30) || K > (1u << 30))
         return sfail(OZA_INVALID_ARG, "oza_server_submit: dimensions must be in [1, 2^30]");
     if (slices < 1 || slices > 20) return sfail(OZA_INVALID_ARG, "oza_server_submit: slices must be in [1, 20]");
     {
-        const oza_status_t chk = oza::check_problem("oza_server_submit", OZA_SCHEME2, M, N, K, slices);
+        const oza_status_t chk = oza::check_problem("oza_server_submit", scheme, M, N, K, slices);
         if (chk != OZA_OK) return chk;
     }
     if (!s || !id) return sfail(OZA_INVALID_ARG, "oza_server_submit: null argument");
     if (!A || !B || !C) return sfail(OZA_INVALID_ARG, "oza_server_submit: null matrix pointer");
-    const size_t bytes = WsLayout(M, N, K, slices).bytes;
+    const size_t bytes = WsLayout(M, N, K, slices, scheme).bytes;
     // The batch block (column maxima, error word) and the batch's device
     // tables (work units: 16 bytes per S x 128 x 256 tile) come from the arena too.
     const size_t batch_extra = align_up(N * 8) + 2 * kAlign + bytes / 1024 + (1u << 20);
@@ -495,6 +511,7 @@ oza_status_t oza_server_submit(oza_server_t s, size_t M, size_t N, size_t K, con
     r->B = B;
     r->C = C;
     r->S = slices;
+    r->scheme = scheme;
     r->ws_bytes = bytes;
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -1,5 +1,7 @@
 // oza_tune_host.cpp -- C ABI of the accuracy tools (see oza_tune.cu):
-// oza_block_error and oza_autotune_slices.
+// oza_block_error, oza_autotune_slices / oza_autotune_scheme (measured on a
+// sampled block) and oza_slices_for_target / oza_scheme_for_target (from the
+// calibrated tables of oza_slice_table.h).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -128,6 +130,64 @@ oza_status_t block_trial(Block& b, int scheme, int slices, double* err) {
     return OZA_OK;
 }
 
+// Smallest S in [1, smax] whose sampled error meets the target, by bisection
+// on the (monotonically falling) error.  *reached = false (and S = smax with
+// its error) if even smax misses.
+oza_status_t bisect_slices(Block& b, int scheme, int smax, double target, int* S, double* err, bool* reached) {
+    double err_hi = 0.0;
+    oza_status_t st = block_trial(b, scheme, smax, &err_hi);
+    if (st != OZA_OK) return st;
+    if (!(err_hi <= target)) {
+        *S = smax;
+        *err = err_hi;
+        *reached = false;
+        return OZA_OK;
+    }
+    int lo = 1, hi = smax;
+    double best = err_hi;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        double e = 0.0;
+        if ((st = block_trial(b, scheme, mid, &e)) != OZA_OK) return st;
+        if (e <= target) {
+            hi = mid;
+            best = e;
+        } else {
+            lo = mid + 1;
+        }
+    }
+    *S = hi;
+    *err = best;
+    *reached = true;
+    return OZA_OK;
+}
+
+// INT8 GEMMs per Ozaki GEMM: S (Scheme II), S (S + 1) / 2 (Scheme I).
+int gemm_count(int scheme, int S) { return scheme == OZA_SCHEME2 ? S : S * (S + 1) / 2; }
+
+// Calibrated-table lookup (oza_slice_table.h) for a target, K and phi.
+template <class Table>
+int table_slices(const Table& tab, double target_rel_err, size_t K, double phi) {
+    // Decade: the smallest d with 10^-d <= target (conservative), clamped to the table.
+    int d = (int)std::ceil(-std::log10(target_rel_err) - 1e-9);
+    if (d < kSliceTableDecadeMin) d = kSliceTableDecadeMin;
+    if (d > kSliceTableDecadeMax) return 21;
+    const int nk = (int)(sizeof(kSliceTableK) / sizeof(kSliceTableK[0]));
+    const int np = (int)(sizeof(kSliceTablePhi) / sizeof(kSliceTablePhi[0]));
+    int ki = 0;
+    while (ki < nk - 1 && (size_t)kSliceTableK[ki] < K) ++ki;
+    int extra = 0;   // beyond the last K: one more slice per factor 4
+    for (size_t k = (size_t)kSliceTableK[nk - 1]; k < K; k *= 4) ++extra;
+    int pi = 0;
+    while (pi < np - 1 && kSliceTablePhi[pi] < phi) ++pi;
+    // Monotone envelope: the measured maximum error is noisy in K and phi.
+    int S = 1;
+    for (int a = 0; a <= ki; ++a)
+        for (int c = 0; c <= pi; ++c) S = std::max(S, (int)tab[a][c][d - kSliceTableDecadeMin]);
+    S += extra;
+    return S > 21 ? 21 : S;
+}
+
 }  // namespace
 
 extern "C" {
@@ -167,57 +227,82 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
     Block b;
     oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
     if (st != OZA_OK) return st;
-    // Smallest S in [1, 20] meeting the target, by bisection on the
-    // (monotonically falling) sampled error, then a check one below.
-    int lo = 1, hi = 20;
-    double err_hi = 0.0;
-    if ((st = block_trial(b, scheme, hi, &err_hi)) != OZA_OK) return st;
-    if (!(err_hi <= target_rel_err)) {
-        *slices = hi;
-        if (achieved_err) *achieved_err = err_hi;
+    int S = 20;
+    double e = 0.0;
+    bool reached = false;
+    if ((st = bisect_slices(b, scheme, 20, target_rel_err, &S, &e, &reached)) != OZA_OK) return st;
+    *slices = S;
+    if (achieved_err) *achieved_err = e;
+    if (!reached) {
         char m[160];
         snprintf(m, sizeof(m), "oza_autotune_slices: target %.3g not reached with 20 slices (sampled error %.3g)",
-                 target_rel_err, err_hi);
+                 target_rel_err, e);
         return tfail(OZA_UNSUPPORTED, m);
     }
-    double best_err = err_hi;
-    while (lo < hi) {
-        const int mid = (lo + hi) / 2;
-        double e = 0.0;
-        if ((st = block_trial(b, scheme, mid, &e)) != OZA_OK) return st;
-        if (e <= target_rel_err) {
-            hi = mid;
-            best_err = e;
-        } else {
-            lo = mid + 1;
-        }
+    return OZA_OK;
+}
+
+oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                                 double target_rel_err, int block, unsigned seed, int* scheme, int* slices,
+                                 double* achieved_err) {
+    if (!ex || !A || !B || !scheme || !slices) return tfail(OZA_INVALID_ARG, "oza_autotune_scheme: null argument");
+    if (!(target_rel_err > 0.0)) return tfail(OZA_INVALID_ARG, "oza_autotune_scheme: target must be > 0");
+    if (M == 0 || N == 0 || K == 0) {
+        *scheme = OZA_SCHEME2;
+        *slices = 1;
+        if (achieved_err) *achieved_err = 0.0;
+        return OZA_OK;
     }
-    if (hi == 20) best_err = err_hi;
-    *slices = hi;
-    if (achieved_err) *achieved_err = best_err;
+    Block b;
+    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
+    if (st != OZA_OK) return st;
+    // Scheme II first (S INT8 GEMMs for S moduli); Scheme I (S (S + 1) / 2
+    // GEMMs) where it is cheaper for the target or where Scheme II's 20
+    // moduli miss it.  Scheme II's moduli are also capped by its INT32 bound.
+    int S2 = 20, S1 = 20;
+    double e2 = 0.0, e1 = 0.0;
+    bool r2 = false, r1 = false;
+    const bool two_ok = (double)K * 125.0 * 125.0 < 2147483648.0;
+    if (two_ok && (st = bisect_slices(b, OZA_SCHEME2, 20, target_rel_err, &S2, &e2, &r2)) != OZA_OK) return st;
+    int s1max = 20;
+    if (r2)
+        while (s1max > 0 && gemm_count(OZA_SCHEME1, s1max) >= S2) --s1max;   // only a cheaper Scheme I counts
+    if (s1max > 0 && (st = bisect_slices(b, OZA_SCHEME1, s1max, target_rel_err, &S1, &e1, &r1)) != OZA_OK) return st;
+    if (r1 || (!r2 && s1max > 0 && (!two_ok || e1 <= e2))) {
+        *scheme = OZA_SCHEME1;
+        *slices = S1;
+        if (achieved_err) *achieved_err = e1;
+    } else {
+        *scheme = OZA_SCHEME2;
+        *slices = S2;
+        if (achieved_err) *achieved_err = e2;
+    }
+    if (!r1 && !r2) {
+        char m[200];
+        snprintf(m, sizeof(m), "oza_autotune_scheme: target %.3g not reached with 20 slices of either scheme "
+                 "(sampled errors %.3g / %.3g)", target_rel_err, e2, e1);
+        return tfail(OZA_UNSUPPORTED, m);
+    }
     return OZA_OK;
 }
 
 int oza_slices_for_target(double target_rel_err, size_t K, double phi) {
     if (!(target_rel_err > 0.0) || K == 0 || !(phi >= 0.0)) return 0;
-    // Decade: the smallest d with 10^-d <= target (conservative), clamped to the table.
-    int d = (int)std::ceil(-std::log10(target_rel_err) - 1e-9);
-    if (d < kSliceTableDecadeMin) d = kSliceTableDecadeMin;
-    if (d > kSliceTableDecadeMax) return 21;
-    const int nk = (int)(sizeof(kSliceTableK) / sizeof(kSliceTableK[0]));
-    const int np = (int)(sizeof(kSliceTablePhi) / sizeof(kSliceTablePhi[0]));
-    int ki = 0;
-    while (ki < nk - 1 && (size_t)kSliceTableK[ki] < K) ++ki;
-    int extra = 0;   // beyond the last K: one more slice per factor 4
-    for (size_t k = (size_t)kSliceTableK[nk - 1]; k < K; k *= 4) ++extra;
-    int pi = 0;
-    while (pi < np - 1 && kSliceTablePhi[pi] < phi) ++pi;
-    // Monotone envelope: the measured maximum error is noisy in K and phi.
-    int S = 1;
-    for (int a = 0; a <= ki; ++a)
-        for (int b = 0; b <= pi; ++b) S = std::max(S, (int)kSliceTable[a][b][d - kSliceTableDecadeMin]);
-    S += extra;
-    return S > 21 ? 21 : S;
+    return table_slices(kSliceTable, target_rel_err, K, phi);
+}
+
+int oza_scheme_for_target(double target_rel_err, size_t K, double phi, int* slices) {
+    if (!slices || !(target_rel_err > 0.0) || K == 0 || !(phi >= 0.0)) return 0;
+    const int s2 = (double)K * 125.0 * 125.0 < 2147483648.0 ? table_slices(kSliceTable, target_rel_err, K, phi) : 21;
+    const int s1 = table_slices(kSliceTable1, target_rel_err, K, phi);
+    // The cheaper in INT8 GEMMs of the schemes that reach the target (Scheme II
+    // on a tie); Scheme I at 20 slices when neither does.
+    if (s2 <= 20 && (s1 > 20 || gemm_count(OZA_SCHEME2, s2) <= gemm_count(OZA_SCHEME1, s1))) {
+        *slices = s2;
+        return OZA_SCHEME2;
+    }
+    *slices = s1;
+    return OZA_SCHEME1;
 }
 
 }  // extern "C"

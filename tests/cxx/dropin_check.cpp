@@ -94,6 +94,19 @@ int main(int argc, char** argv) {
         std::printf("ok scheme2 S=%d total_ms=%.3f\n", S2, t.total_ms);
     }
     {
+        // Extension: the reference's buffer layouts from the getters.
+        ozablas::WorkspaceScheme2 ws(exec, M, N, K, S2, ozablas::WorkspaceLayout::Reference);
+        ozablas::ozaki_scheme2_gemm(ws, dA, dB, dC);
+        exec->synchronize();
+        std::vector<int8_t> sl((size_t)S2 * M * K);
+        exec->copy_to_host(sl.data(), ws.get_A_slices(), sl.size());
+        write_file(dir + "/A2_slices.bin", sl.data(), sl.size());
+        std::vector<int8_t> slb((size_t)S2 * K * N);
+        exec->copy_to_host(slb.data(), ws.get_B_slices(), slb.size());
+        write_file(dir + "/B2_slices.bin", slb.data(), slb.size());
+        std::printf("ok reference layout\n");
+    }
+    {
         ozablas::WorkspaceScheme1 ws(exec, M, N, K, S1);
         ozablas::ozaki_scheme1_gemm(ws, dA, dB, dC);
         exec->synchronize();

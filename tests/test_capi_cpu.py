@@ -161,7 +161,7 @@ def test_scheme2_int32_bound_enforced_by_every_entry_point(K, want):
     rid = ctypes.c_uint64()
     results = {
         "group": L.oza_group_create(None, 2, 1, one(8), one(8), one(K), s, 0, ctypes.byref(h)),
-        "server": L.oza_server_submit(None, 8, 8, K, None, None, None, 4, ctypes.byref(rid)),
+        "server": L.oza_server_submit(None, 2, 8, 8, K, None, None, None, 4, ctypes.byref(rid)),
         "noalloc": L.oza_gemm_noalloc(2, 4, 8, 8, K, None, None, None, None),
     }
     for name, st in results.items():
@@ -187,12 +187,35 @@ def test_shared_check_rejects_slice_counts_and_tma_extents():
     assert "too large" in L.oza_last_error_string().decode()
 
 
+def test_scheme_for_target_picks_the_cheaper_scheme_that_reaches():
+    """oza_scheme_for_target: Scheme II whenever its table reaches the target
+    with no more INT8 GEMMs than Scheme I's; otherwise Scheme I (its count from
+    its own calibrated table); 21 when neither reaches it."""
+    for t in (1e-9, 1e-12, 1e-14, 1e-15, 1e-16):
+        for K in (128, 1024, 8192, 65536, 200000):
+            for phi in (0.5, 1.0, 2.0, 4.0):
+                sc, S = oz.scheme_for_target(t, K, phi)
+                assert sc in (1, 2) and 1 <= S <= 21
+                s2 = oz.slices_for_target(t, K, phi) if K <= 137438 else 21
+                if sc == 2:
+                    assert S == s2 <= 20
+                else:
+                    assert s2 > 20 or S * (S + 1) // 2 < s2
+    # wide exponent range and tight target: Scheme II's 20 moduli run out
+    assert oz.scheme_for_target(1e-15, 16384, 4.0)[0] == 1
+    # easy target: Scheme II
+    assert oz.scheme_for_target(1e-9, 1024, 0.5)[0] == 2
+    with pytest.raises(ValueError):
+        oz.scheme_for_target(0.0, 1024, 1.0)
+
+
 def test_server_api_without_a_device():
     L = oz.lib()
     h = ctypes.c_void_p()
     assert L.oza_server_create(None, None, ctypes.byref(h)) == oz.OZA_INVALID_ARG
     rid = ctypes.c_uint64()
-    assert L.oza_server_submit(None, 4, 4, 4, None, None, None, 8, ctypes.byref(rid)) == oz.OZA_INVALID_ARG
+    assert L.oza_server_submit(None, 2, 4, 4, 4, None, None, None, 8, ctypes.byref(rid)) == oz.OZA_INVALID_ARG
+    assert L.oza_server_submit(None, 3, 4, 4, 4, None, None, None, 8, ctypes.byref(rid)) == oz.OZA_INVALID_ARG
     assert L.oza_server_destroy(None) == oz.OZA_OK
 
 
@@ -204,6 +227,8 @@ def test_server_request_bytes_layout():
         Mp, Np, Kp = ru(M, 128), ru(N, 256), ru(K, 128)
         want = sum(ru(x, 1024) for x in (4 * M, 4 * N, S * Mp * Kp, S * Np * Kp, S * Mp * Np))
         assert oz.Server.request_bytes(M, N, K, S) == want
+        want1 = sum(ru(x, 1024) for x in (4 * M, 4 * N, S * Mp * Kp, S * Np * Kp, 4 * S * Mp * Np))
+        assert oz.Server.request_bytes(M, N, K, S, scheme=1) == want1
     assert oz.Server.request_bytes(0, 4, 4, 8) == 0
     assert oz.Server.request_bytes(4, 4, 4, 21) == 0
 

@@ -53,6 +53,10 @@ def test_cxx_program_on_drop_in_headers_matches_oracle(tmp_path):
         assert np.array_equal(bits(got), bits(ref["C"])), name
     sh = np.fromfile(tmp_path / "shiftA2.bin", dtype=np.int32)
     assert np.array_equal(sh, ref2["shift_A"])
+    sl = np.fromfile(tmp_path / "A2_slices.bin", dtype=np.int8).reshape(S2, M, K)
+    assert np.array_equal(sl, ref2["A_slices"])
+    slb = np.fromfile(tmp_path / "B2_slices.bin", dtype=np.int8).reshape(S2, K, N)
+    assert np.array_equal(slb, ref2["B_slices"])
 
 
 def test_reference_scheme2_example_runs_on_this_library():

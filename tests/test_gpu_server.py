@@ -117,3 +117,34 @@ def test_wait_timeout_then_completion(executor):
         st = srv.wait(rid, timeout=120)
         assert st["status"] == 0 and st["slices"] == 16
     assert _same(C, _alone(executor, A, B, 16))
+
+
+def _alone_scheme(executor, scheme, A, B, S):
+    import torch
+    M, K = A.shape
+    N = B.shape[1]
+    C = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    if scheme == 2:
+        oz.ozaki_scheme2_gemm(oz.WorkspaceScheme2(executor, M, N, K, S), A, B, C)
+    else:
+        oz.ozaki_scheme1_gemm(oz.WorkspaceScheme1(executor, M, N, K, S), A, B, C)
+    torch.cuda.synchronize()
+    return C
+
+
+def test_scheme_i_requests_in_the_mix(executor):
+    """Requests for which the accuracy knob chose Scheme I run as batches of
+    their own among batched Scheme II requests; every result equals its
+    scheme's oza_gemm alone, bit for bit."""
+    reqs = [(300, 200, 500, 2, 16), (257, 129, 1000, 1, 11), (90, 400, 300, 2, 18), (128, 256, 640, 2, 12),
+            (500, 70, 2000, 1, 8), (64, 64, 64, 2, 20), (200, 300, 400, 1, 13), (330, 220, 110, 2, 9)]
+    data = [_req(M, N, K, 2.0, 9000 + 2 * i) for i, (M, N, K, _, _) in enumerate(reqs)]
+    with oz.Server(executor, 2 << 30, max_inflight=2, max_batch=8) as srv:
+        ids = [srv.submit(A, B, C, S, scheme=sc) for (A, B, C), (_, _, _, sc, S) in zip(data, reqs)]
+        stats = [srv.wait(i, timeout=120) for i in ids]
+    for st, (_, _, _, sc, _) in zip(stats, reqs):
+        assert st["status"] == 0
+        if sc == 1:
+            assert st["batch_size"] == 1
+    for (A, B, C), (_, _, _, sc, S) in zip(data, reqs):
+        assert _same(C, _alone_scheme(executor, sc, A, B, S)), (sc, S)

@@ -63,3 +63,35 @@ def test_scheme2_4096_matches_reference_gpu(executor):
     ref = ref_gpu.run(executor, 2, A, B, 16)
     got = run_pipeline(oz, executor, 2, A, B, 16, materialize=False)
     assert np.array_equal(bits(got["C"]), bits(ref["C"]))
+
+
+@pytest.mark.parametrize("scheme,S", [(2, 12), (1, 6)])
+def test_reference_layout_getters_match_reference_buffers(executor, scheme, S):
+    """With OZA_WS_REFERENCE_LAYOUT the workspace getters return the
+    reference's own layouts, byte for byte what the reference's getters
+    (workspace.hpp:14-94) return after the same call: A slices [S][M][K],
+    B slices [S][K][N], C_tc [S][M][N] (Scheme II) or the last group (Scheme I)."""
+    import ctypes
+    import torch
+    oz = _oz()
+    M, N, K = 300, 200, 333
+    A = oz.generate_matrix(M, K, 1.0, 42)
+    B = oz.generate_matrix(K, N, 1.0, 43)
+    ref = ref_gpu.run(executor, scheme, A, B, S)
+    ws = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(executor, M, N, K, S, reference_layout=True)
+    dC = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    (oz.ozaki_scheme2_gemm if scheme == 2 else oz.ozaki_scheme1_gemm)(
+        ws, torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda(), dC)
+    torch.cuda.synchronize()
+
+    def grab(ptr, shape, dtype):
+        a = np.empty(shape, dtype)
+        executor.copy_to_host(a.ctypes.data_as(ctypes.c_void_p).value, ptr, a.nbytes)
+        return a
+
+    G = S if scheme == 2 else 1
+    assert np.array_equal(grab(ws.get_A_slices(), (S, M, K), np.int8), ref["A_slices"])
+    assert np.array_equal(grab(ws.get_B_slices(), (S, K, N), np.int8), ref["B_slices"])
+    assert np.array_equal(grab(ws.get_C_tc(), (G, M, N), np.int32), ref["C_tc"])
+    assert np.array_equal(grab(ws.get_shift_A(), (M,), np.int32), ref["shift_A"])
+    assert np.array_equal(bits(dC.cpu().numpy()), bits(ref["C"]))
