@@ -723,16 +723,21 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
 // drift across all S planes and re-read them from HBM (4.6x at 8192^3, S=16).
 //   warp 0      TMA producer (4-stage ring of A 128x128 + B^T 256x128 int8 tiles)
 //   warp 1      TMEM allocation, UMMA issue (one elected lane)
-//   warps 2..5  epilogue; warp w reads TMEM lanes 32 (w % 4).. (its lane
-//               quadrant), all 256 columns in two halves.  Four warps measured
-//               1-2% faster GEMMs than eight (one warp per quadrant and half).
+//   warps 2..   epilogue, EW warps; warp w reads TMEM lanes 32 (w % 4).. (its
+//               lane quadrant): with EW = 4 all 256 columns in two halves, with
+//               EW = 8 the column half (w - 2) / 4.  Four warps measured 1-2%
+//               faster at large K (the epilogue hides behind a unit's MMAs);
+//               units of few k-blocks, where the epilogue is the longer side,
+//               take eight.
 // Epilogues: kEpiI32 writes the INT32 group planes; kEpiCoef (Scheme II)
 // reduces each residue product to its one-byte CRT coefficient and writes the
 // byte planes, which k_crt_coef turns into FP64 C (a quarter of the INT32
 // traffic, and the multiword CRT runs at full occupancy instead of in the
 // epilogue warps, where it would stall the MMA pipeline).
-constexpr int kEpiWarps = 4;
-constexpr int kGemmThreads = 64 + 32 * kEpiWarps;
+template <int EW>
+constexpr int gemm_threads() { return 64 + 32 * EW; }
+// Units with fewer k-blocks of MMAs than this get 8 epilogue warps.
+constexpr int kEpi8Below = 8;
 constexpr int kStages = 4;
 constexpr int kABytes = kTileM * kTileK;   // 16 KB per stage
 constexpr int kBBytes = kTileN * kTileK;   // 32 KB per stage
@@ -892,8 +897,9 @@ struct GroupUnits {
 // TMA loads into a kStages ring, warp 1 issues tcgen05 MMAs into one of two
 // TMEM accumulators, warps 2-9 drain the other accumulator through the
 // epilogue.  CTA c takes units c, c + grid, ...  Every wait is bounded.
-template <int EPI, class Units>
+template <int EPI, int EW, class Units>
 __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_t hint) {
+    static_assert(EW == 4 || EW == 8, "4 or 8 epilogue warps");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
@@ -914,8 +920,8 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
         }
         mbar_init(&acc_full[0], 1);
         mbar_init(&acc_full[1], 1);
-        mbar_init(&acc_empty[0], kEpiWarps);
-        mbar_init(&acc_empty[1], kEpiWarps);
+        mbar_init(&acc_empty[0], EW);
+        mbar_init(&acc_empty[1], EW);
         mbar_init(drain, 1);
         *abort_flag = 0;
         fence_barrier_init();
@@ -1034,6 +1040,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3;                 // TMEM lane quadrant this warp may access
+        const int h0 = EW == 8 ? (warp - 2) >> 2 : 0, h1 = EW == 8 ? h0 + 1 : 2;   // column halves
         const int row_local = q * 32 + lane;
         int local = 0;
         bool ok = true;
@@ -1050,7 +1057,7 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
                 continue;
             }
             tc_fence_after();
-            for (int half = 0; half < 2; ++half) {
+            for (int half = h0; half < h1; ++half) {
                 const uint32_t taddr =
                     tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
                 epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, half);
@@ -1069,18 +1076,19 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
     }
 }
 
-template <int EPI>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+template <int EPI, int EW>
+__global__ void __launch_bounds__(gemm_threads<EW>(), 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const __grid_constant__ PairList pairs, const __grid_constant__ GemmArgs args) {
     const SingleUnits src{&tmA, &tmB, &pairs, &args};
-    gemm_i8_body<EPI>(src, args.err, args.wait_hint);
+    gemm_i8_body<EPI, EW>(src, args.err, args.wait_hint);
 }
 
 // Grouped Scheme II GEMM over an explicit unit list (coefficient epilogue).
-__global__ void __launch_bounds__(kGemmThreads, 1) k_group_gemm_i8(const __grid_constant__ GroupGemmArgs g) {
+// Grouped problems are mostly of small K: eight epilogue warps.
+__global__ void __launch_bounds__(gemm_threads<8>(), 1) k_group_gemm_i8(const __grid_constant__ GroupGemmArgs g) {
     const GroupUnits src{&g};
-    gemm_i8_body<kEpiCoef>(src, g.err, g.wait_hint);
+    gemm_i8_body<kEpiCoef, 8>(src, g.err, g.wait_hint);
 }
 
 // ---------------------------------------------------------------------------
@@ -1542,16 +1550,16 @@ cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, c
     return cudaGetLastError();
 }
 
-template <int EPI>
+template <int EPI, int EW>
 static cudaError_t gemm_launch(const CUtensorMap& tmA, const CUtensorMap& tmB, const PairList& pairs,
                                const GemmArgs& a, int grid, cudaStream_t st) {
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_gemm_i8<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        attr = cudaFuncSetAttribute(k_gemm_i8<EPI, EW>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
     });
     if (attr != cudaSuccess) return attr;
-    k_gemm_i8<EPI><<<grid, kGemmThreads, kGemmSmem, st>>>(tmA, tmB, pairs, a);
+    k_gemm_i8<EPI, EW><<<grid, gemm_threads<EW>(), kGemmSmem, st>>>(tmA, tmB, pairs, a);
     return cudaGetLastError();
 }
 
@@ -1583,8 +1591,13 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     const long long units = (long long)a.total_tiles * a.groups;
     if (units == 0) return cudaSuccess;
     const int grid = (int)(units < p.sms ? units : p.sms);
-    return p.coef ? gemm_launch<kEpiCoef>(tmA, tmB, p.pairs, a, grid, st)
-                  : gemm_launch<kEpiI32>(tmA, tmB, p.pairs, a, grid, st);
+    // k-blocks of MMAs per unit, averaged over the groups (Scheme I groups sum several pairs)
+    const long long unit_kb = (long long)a.k_blocks * p.pairs.start[a.groups] / a.groups;
+    if (unit_kb < kEpi8Below)
+        return p.coef ? gemm_launch<kEpiCoef, 8>(tmA, tmB, p.pairs, a, grid, st)
+                      : gemm_launch<kEpiI32, 8>(tmA, tmB, p.pairs, a, grid, st);
+    return p.coef ? gemm_launch<kEpiCoef, 4>(tmA, tmB, p.pairs, a, grid, st)
+                  : gemm_launch<kEpiI32, 4>(tmA, tmB, p.pairs, a, grid, st);
 }
 
 cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S,
@@ -1911,7 +1924,7 @@ cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t c
     }
     if (ev) OZA_TRY(cudaEventRecord(ev[2], st));
     const int grid = p->gemm.total_units < sms ? p->gemm.total_units : sms;
-    if (grid > 0) k_group_gemm_i8<<<grid, kGemmThreads, kGemmSmem, st>>>(p->gemm);
+    if (grid > 0) k_group_gemm_i8<<<grid, gemm_threads<8>(), kGemmSmem, st>>>(p->gemm);
     OZA_TRY(cudaGetLastError());
     if (ev) OZA_TRY(cudaEventRecord(ev[3], st));
     for (const GroupPlan::Launch& L : p->crt) {
