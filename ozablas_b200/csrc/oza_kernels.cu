@@ -305,6 +305,26 @@ __global__ void __launch_bounds__(256) k_stats_cols(const double* __restrict__ B
     stats_cols_block(B, rows, cols, colmax, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
+// Position (row, chunk) of a grid-stride walk over rows x chunks, advanced by
+// a fixed stride with one compare instead of a 64-bit division per step.
+struct GridWalk {
+    long long r, c, dr, dc, chunks;
+    __device__ __forceinline__ GridWalk(long long start, long long stride, long long chunks_) : chunks(chunks_) {
+        r = start / chunks;
+        c = start - r * chunks;
+        dr = stride / chunks;
+        dc = stride - dr * chunks;
+    }
+    __device__ __forceinline__ void next() {
+        r += dr;
+        c += dc;
+        if (c >= chunks) {
+            c -= chunks;
+            ++r;
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Step 2: slicing
 // ---------------------------------------------------------------------------
@@ -489,17 +509,15 @@ __device__ __forceinline__ bool store_if_zero(const double (&v)[E], int planes, 
 // A (rows x cols, row-major) -> out[s][rows_p][cols_p].  One thread per E
 // consecutive columns of a row (E = 8 for Scheme II, 8-byte stores per plane;
 // 16 for Scheme I), coalesced.  Scheme II is instantiated per slice count SC
-// (= S); Scheme I takes S at run time.  `id` is the chunk index over the
-// padded rows_p x (cols_p / E) chunks.
+// (= S); Scheme I takes S at run time.  (r, ch) is the chunk's row and its
+// index among the row's cols_p / E chunks.
 template <int SCHEME, int SC, bool WIDE>
 __device__ __forceinline__ void slice_rows_chunk(const double* __restrict__ A, long long rows, long long cols,
                                                  const int32_t* __restrict__ shift, int S, int beta,
                                                  int8_t* __restrict__ out, long long cols_p, size_t plane,
-                                                 long long id) {
+                                                 long long r, long long ch) {
     constexpr int E = SCHEME == 2 ? 8 : 16;
-    const long long chunks_per_row = cols_p / E;
-    const long long r = id / chunks_per_row;
-    const long long c0 = (id - r * chunks_per_row) * E;
+    const long long c0 = ch * E;
     double v[E];
     int sh = 0;
     if (r < rows) {
@@ -526,11 +544,10 @@ __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_rows(
     const double* __restrict__ A, long long rows, long long cols, const int32_t* __restrict__ shift, int S, int beta,
     int8_t* __restrict__ out, long long rows_p, long long cols_p, long long plane_rows) {
     constexpr int E = SCHEME == 2 ? 8 : 16;
-    const long long total = rows_p * (cols_p / E);
     const size_t plane = (size_t)plane_rows * (size_t)cols_p;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x)
-        slice_rows_chunk<SCHEME, SC, WIDE>(A, rows, cols, shift, S, beta, out, cols_p, plane, id);
+    for (GridWalk w((long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, cols_p / E);
+         w.r < rows_p; w.next())
+        slice_rows_chunk<SCHEME, SC, WIDE>(A, rows, cols, shift, S, beta, out, cols_p, plane, w.r, w.c);
 }
 
 // B (K x N, row-major) -> out[s][Np][Kp], i.e. B^T, K-major.  Tile (bx, by) of
@@ -1107,11 +1124,11 @@ template <int S>
 __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef, long long Np, long long N,
                                                size_t plane, const int32_t* __restrict__ sA,
                                                const int32_t* __restrict__ sB, double* __restrict__ C,
-                                               long long chunks, long long id) {
+                                               long long i, long long ch) {
     constexpr int NL = (S + 3) / 4;   // 32-bit limbs of M
     constexpr int NT = S / 3;         // residue triples
     const CrtTable& T = c_crt[S - 1];
-    const long long i = id / chunks, j0 = (id - i * chunks) << 2;
+    const long long j0 = ch << 2;
     const uint8_t* src = coef + (size_t)i * Np + j0;
     uint32_t w[S];
 #pragma unroll
@@ -1158,12 +1175,10 @@ template <int S>
 __global__ void __launch_bounds__(128) k_crt_coef(const uint8_t* __restrict__ coef, long long Mp, long long Np,
                                                   long long M, long long N, const int32_t* __restrict__ sA,
                                                   const int32_t* __restrict__ sB, double* __restrict__ C) {
-    const long long chunks = (N + 3) >> 2;
-    const long long total = M * chunks;
     const size_t plane = (size_t)Mp * (size_t)Np;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x)
-        crt_coef_chunk<S>(coef, Np, N, plane, sA, sB, C, chunks, id);
+    for (GridWalk w((long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, (N + 3) >> 2);
+         w.r < M; w.next())
+        crt_coef_chunk<S>(coef, Np, N, plane, sA, sB, C, w.r, w.c);
 }
 
 template <int NL>
@@ -1207,9 +1222,9 @@ template <int S>
 __device__ __forceinline__ void reconstruct1_chunk(const int32_t* __restrict__ ctc, long long Np, long long N,
                                                    size_t plane, int beta, const int32_t* __restrict__ negA,
                                                    const int32_t* __restrict__ negB, double* __restrict__ C,
-                                                   long long chunks, long long id) {
+                                                   long long i, long long ch) {
     constexpr int kBatch = 4;   // group planes loaded together
-    const long long i = id / chunks, j0 = (id - i * chunks) << 2;
+    const long long j0 = ch << 2;
     const int4* src = reinterpret_cast<const int4*>(ctc + (size_t)i * Np + j0);
     const size_t plane4 = plane >> 2;
     int4 v[kBatch];
@@ -1260,12 +1275,10 @@ __global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict_
                                                       long long M, long long N, int beta,
                                                       const int32_t* __restrict__ negA,
                                                       const int32_t* __restrict__ negB, double* __restrict__ C) {
-    const long long chunks = (N + 3) >> 2;
-    const long long total = M * chunks;
     const size_t plane = (size_t)Mp * (size_t)Np;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (long long)gridDim.x * blockDim.x)
-        reconstruct1_chunk<S>(ctc, Np, N, plane, beta, negA, negB, C, chunks, id);
+    for (GridWalk w((long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, (N + 3) >> 2);
+         w.r < M; w.next())
+        reconstruct1_chunk<S>(ctc, Np, N, plane, beta, negA, negB, C, w.r, w.c);
 }
 
 // ---------------------------------------------------------------------------
@@ -1345,8 +1358,9 @@ __global__ void __launch_bounds__(256, 3) k_group_slice_rows(const GroupProblemD
     for (int r = 0; r < kGroupRowChunks; ++r) {
         const long long id = base + r * 256;
         if (id >= total) return;
+        const long long cpr = P.Kp / 8;
         slice_rows_chunk<2, SC, WIDE>(P.A, P.M, P.K, P.shiftA, SC, 0, P.a_planes, P.Kp,
-                                      (size_t)P.Mp * (size_t)P.Kp, id);
+                                      (size_t)P.Mp * (size_t)P.Kp, id / cpr, id % cpr);
     }
 }
 
@@ -1377,7 +1391,8 @@ __global__ void __launch_bounds__(256) k_group_crt(const GroupProblemDev* __rest
     const long long chunks = (P.N + 3) >> 2;
     const long long id = (blockIdx.x - L.start[q]) * 256 + threadIdx.x;
     if (id >= P.M * chunks) return;
-    crt_coef_chunk<S>(P.coef, P.Np, P.N, (size_t)P.Mp * (size_t)P.Np, P.shiftA, P.shiftB, P.C, chunks, id);
+    crt_coef_chunk<S>(P.coef, P.Np, P.N, (size_t)P.Mp * (size_t)P.Np, P.shiftA, P.shiftB, P.C, id / chunks,
+                      id % chunks);
 }
 
 // ---------------------------------------------------------------------------
