@@ -320,7 +320,9 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
 
 /* The accuracy knob's choice of scheme as well: Scheme II (S INT8 GEMMs for
  * S moduli) or Scheme I (S (S + 1) / 2 GEMMs for S slices), whichever meets
- * `target_rel_err` on the seeded block sample with fewer INT8 GEMMs --
+ * `target_rel_err` with fewer INT8 GEMMs on two independent seeded block
+ * samples (`seed` and a second seed derived from it; the count must meet the
+ * target on both) --
  * Scheme I where Scheme II's 20 moduli miss the target (wide exponent ranges,
  * deep K) or where K exceeds Scheme II's INT32-exact bound.  Returns
  * OZA_UNSUPPORTED, with the scheme whose 20-slice error is lower, if neither

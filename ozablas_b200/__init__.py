@@ -591,9 +591,10 @@ def autotune_slices(executor, scheme: int, A, B, M: int, N: int, K: int, target_
 
 def autotune_scheme(executor, A, B, M: int, N: int, K: int, target_rel_err: float, block: int = 96,
                     seed: int = 7):
-    """Scheme and slice count meeting target_rel_err on a sampled block with the
-    fewest INT8 GEMMs (Scheme I where Scheme II's 20 moduli miss it); returns
-    (scheme, slices, sampled error).  Raises OzaError if neither scheme reaches it."""
+    """Scheme and slice count meeting target_rel_err with the fewest INT8 GEMMs
+    on two independent sampled blocks (Scheme I where Scheme II's 20 moduli
+    miss it); returns (scheme, slices, largest sampled error).  Raises OzaError
+    if neither scheme reaches it."""
     sc, s = ctypes.c_int(), ctypes.c_int()
     e = ctypes.c_double()
     _check(lib().oza_autotune_scheme(executor.handle, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),

@@ -130,12 +130,26 @@ oza_status_t block_trial(Block& b, int scheme, int slices, double* err) {
     return OZA_OK;
 }
 
-// Smallest S in [1, smax] whose sampled error meets the target, by bisection
-// on the (monotonically falling) error.  *reached = false (and S = smax with
-// its error) if even smax misses.
-oza_status_t bisect_slices(Block& b, int scheme, int smax, double target, int* S, double* err, bool* reached) {
+// The largest sampled error over several blocks.
+oza_status_t blocks_trial(Block* const* blocks, int nblocks, int scheme, int slices, double* err) {
+    double worst = 0.0;
+    for (int i = 0; i < nblocks; ++i) {
+        double e = 0.0;
+        const oza_status_t st = block_trial(*blocks[i], scheme, slices, &e);
+        if (st != OZA_OK) return st;
+        if (!(e <= worst)) worst = e;   // NaN propagates
+    }
+    *err = worst;
+    return OZA_OK;
+}
+
+// Smallest S in [1, smax] whose sampled error (the largest over the blocks)
+// meets the target, by bisection on the (monotonically falling) error.
+// *reached = false (and S = smax with its error) if even smax misses.
+oza_status_t bisect_slices(Block* const* blocks, int nblocks, int scheme, int smax, double target, int* S,
+                           double* err, bool* reached) {
     double err_hi = 0.0;
-    oza_status_t st = block_trial(b, scheme, smax, &err_hi);
+    oza_status_t st = blocks_trial(blocks, nblocks, scheme, smax, &err_hi);
     if (st != OZA_OK) return st;
     if (!(err_hi <= target)) {
         *S = smax;
@@ -148,7 +162,7 @@ oza_status_t bisect_slices(Block& b, int scheme, int smax, double target, int* S
     while (lo < hi) {
         const int mid = (lo + hi) / 2;
         double e = 0.0;
-        if ((st = block_trial(b, scheme, mid, &e)) != OZA_OK) return st;
+        if ((st = blocks_trial(blocks, nblocks, scheme, mid, &e)) != OZA_OK) return st;
         if (e <= target) {
             hi = mid;
             best = e;
@@ -230,7 +244,8 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
     int S = 20;
     double e = 0.0;
     bool reached = false;
-    if ((st = bisect_slices(b, scheme, 20, target_rel_err, &S, &e, &reached)) != OZA_OK) return st;
+    Block* blocks[1] = {&b};
+    if ((st = bisect_slices(blocks, 1, scheme, 20, target_rel_err, &S, &e, &reached)) != OZA_OK) return st;
     *slices = S;
     if (achieved_err) *achieved_err = e;
     if (!reached) {
@@ -253,9 +268,14 @@ oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, co
         if (achieved_err) *achieved_err = 0.0;
         return OZA_OK;
     }
-    Block b;
-    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
+    // Two independent seeded blocks: a count is accepted only if it meets the
+    // target on both, so a count that just reaches it on one sample (the
+    // largest error over many outputs is heavy-tailed) is not taken.
+    Block b0, b1;
+    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b0);
+    if (st == OZA_OK) st = make_block(ex, A, B, M, N, K, block, seed ^ 0x5bd1e995u, b1);
     if (st != OZA_OK) return st;
+    Block* blocks[2] = {&b0, &b1};
     // Scheme II first (S INT8 GEMMs for S moduli); Scheme I (S (S + 1) / 2
     // GEMMs) where it is cheaper for the target or where Scheme II's 20
     // moduli miss it.  Scheme II's moduli are also capped by its INT32 bound.
@@ -263,11 +283,13 @@ oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, co
     double e2 = 0.0, e1 = 0.0;
     bool r2 = false, r1 = false;
     const bool two_ok = (double)K * 125.0 * 125.0 < 2147483648.0;
-    if (two_ok && (st = bisect_slices(b, OZA_SCHEME2, 20, target_rel_err, &S2, &e2, &r2)) != OZA_OK) return st;
+    if (two_ok && (st = bisect_slices(blocks, 2, OZA_SCHEME2, 20, target_rel_err, &S2, &e2, &r2)) != OZA_OK)
+        return st;
     int s1max = 20;
     if (r2)
         while (s1max > 0 && gemm_count(OZA_SCHEME1, s1max) >= S2) --s1max;   // only a cheaper Scheme I counts
-    if (s1max > 0 && (st = bisect_slices(b, OZA_SCHEME1, s1max, target_rel_err, &S1, &e1, &r1)) != OZA_OK) return st;
+    if (s1max > 0 && (st = bisect_slices(blocks, 2, OZA_SCHEME1, s1max, target_rel_err, &S1, &e1, &r1)) != OZA_OK)
+        return st;
     if (r1 || (!r2 && s1max > 0 && (!two_ok || e1 <= e2))) {
         *scheme = OZA_SCHEME1;
         *slices = S1;

@@ -109,28 +109,29 @@ def test_autotune_argument_checks(executor):
         oz.block_error(executor, A, A, A, 4, 4, 4, block=0)
 
 
-def test_autotune_scheme_switches_to_scheme_i_where_moduli_run_out(executor):
-    """phi = 4 with deep K: 20 moduli leave errors near 1e-9 on such inputs,
-    so for a 1e-12 target the knob picks Scheme I and its count meets it."""
-    M, N, K = 128, 128, 16384
-    A = oz.generate_matrix(M, K, phi=4.0, seed=51)
-    B = oz.generate_matrix(K, N, phi=4.0, seed=52)
+@pytest.mark.parametrize("K,phi,target", [(16384, 4.0, 1e-14), (140000, 1.0, 1e-12), (2048, 0.5, 1e-12)])
+def test_autotune_scheme_choice(executor, K, phi, target):
+    """oza_autotune_scheme takes Scheme II where its moduli meet the target on
+    both sampled blocks (the same count as the single-scheme autotuner with
+    both blocks' worst error), Scheme I where they do not -- for a wide
+    exponent range with a tight target, and always beyond Scheme II's INT32
+    bound (K > 137438) -- and its count then meets the target."""
+    M, N = 128, 128
+    A = oz.generate_matrix(M, K, phi=phi, seed=51)
+    B = oz.generate_matrix(K, N, phi=phi, seed=52)
     dA, dB = _dev(A), _dev(B)
-    target = 1e-12
     scheme, S, err = oz.autotune_scheme(executor, dA, dB, M, N, K, target, block=64, seed=3)
-    assert scheme == 1 and 1 <= S <= 20 and err <= target
-    with pytest.raises(oz.OzaError):
-        oz.autotune_slices(executor, 2, dA, dB, M, N, K, target, block=64, seed=3)
-    C = _run(executor, 1, A, B, S)
-    assert oz.block_error(executor, dA, dB, _dev(C), M, N, K, block=64, seed=3) == pytest.approx(err, abs=0)
-
-
-def test_autotune_scheme_keeps_scheme_ii_where_it_reaches(executor):
-    M, N, K = 256, 200, 512
-    A = oz.generate_matrix(M, K, phi=0.5, seed=61)
-    B = oz.generate_matrix(K, N, phi=0.5, seed=62)
-    dA, dB = _dev(A), _dev(B)
-    target = 1e-12
-    scheme, S, err = oz.autotune_scheme(executor, dA, dB, M, N, K, target, block=96, seed=4)
-    S2, e2 = oz.autotune_slices(executor, 2, dA, dB, M, N, K, target, block=96, seed=4)
-    assert (scheme, S, err) == (2, S2, e2)
+    assert 1 <= S <= 20 and err <= target
+    C = _run(executor, scheme, A, B, S)
+    for sd in (3, 3 ^ 0x5bd1e995):
+        assert oz.block_error(executor, dA, dB, _dev(C), M, N, K, block=64, seed=sd) <= target
+    if K > 137438:
+        assert scheme == 1
+        return
+    # Scheme II at 20 moduli on the same two blocks decides which scheme is due
+    C20 = _run(executor, 2, A, B, 20)
+    e20 = max(oz.block_error(executor, dA, dB, _dev(C20), M, N, K, block=64, seed=sd) for sd in (3, 3 ^ 0x5bd1e995))
+    if e20 > target:
+        assert scheme == 1
+    else:
+        assert scheme == 2 or S * (S + 1) // 2 < 20

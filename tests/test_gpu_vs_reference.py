@@ -74,7 +74,9 @@ def test_reference_layout_getters_match_reference_buffers(executor, scheme, S):
     import ctypes
     import torch
     oz = _oz()
-    M, N, K = 300, 200, 333
+    # sizes the reference's cuBLAS INT8 GEMMs accept (it does not check their
+    # status; with K = 333 they refuse and its C_tc stays zero)
+    M, N, K = 320, 192, 352
     A = oz.generate_matrix(M, K, 1.0, 42)
     B = oz.generate_matrix(K, N, 1.0, 43)
     ref = ref_gpu.run(executor, scheme, A, B, S)
