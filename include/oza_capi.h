@@ -322,7 +322,7 @@ oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, 
  * S moduli) or Scheme I (S (S + 1) / 2 GEMMs for S slices), whichever meets
  * `target_rel_err` with fewer INT8 GEMMs on two independent seeded block
  * samples (`seed` and a second seed derived from it; the count must meet the
- * target on both) --
+ * target on both; Scheme II at its 20-modulus cap on four more) --
  * Scheme I where Scheme II's 20 moduli miss the target (wide exponent ranges,
  * deep K) or where K exceeds Scheme II's INT32-exact bound.  Returns
  * OZA_UNSUPPORTED, with the scheme whose 20-slice error is lower, if neither

@@ -285,6 +285,19 @@ oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, co
     const bool two_ok = (double)K * 125.0 * 125.0 < 2147483648.0;
     if (two_ok && (st = bisect_slices(blocks, 2, OZA_SCHEME2, 20, target_rel_err, &S2, &e2, &r2)) != OZA_OK)
         return st;
+    if (r2 && S2 == 20) {
+        // Scheme II reaches the target only at its last modulus, with no count
+        // left to add: confirm on four more blocks before taking it (the
+        // largest relative error over many outputs is heavy-tailed).
+        for (unsigned k = 1; k <= 4 && r2; ++k) {
+            Block extra;
+            if ((st = make_block(ex, A, B, M, N, K, block, seed + 0x9e3779b9u * k, extra)) != OZA_OK) return st;
+            double e = 0.0;
+            if ((st = block_trial(extra, OZA_SCHEME2, 20, &e)) != OZA_OK) return st;
+            if (!(e <= e2)) e2 = e;
+            r2 = e2 <= target_rel_err;
+        }
+    }
     int s1max = 20;
     if (r2)
         while (s1max > 0 && gemm_count(OZA_SCHEME1, s1max) >= S2) --s1max;   // only a cheaper Scheme I counts

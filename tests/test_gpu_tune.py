@@ -112,10 +112,9 @@ def test_autotune_argument_checks(executor):
 @pytest.mark.parametrize("K,phi,target", [(16384, 4.0, 1e-14), (140000, 1.0, 1e-12), (2048, 0.5, 1e-12)])
 def test_autotune_scheme_choice(executor, K, phi, target):
     """oza_autotune_scheme takes Scheme II where its moduli meet the target on
-    both sampled blocks (the same count as the single-scheme autotuner with
-    both blocks' worst error), Scheme I where they do not -- for a wide
-    exponent range with a tight target, and always beyond Scheme II's INT32
-    bound (K > 137438) -- and its count then meets the target."""
+    both sampled blocks, Scheme I where they do not -- for a wide exponent
+    range with a tight target, and always beyond Scheme II's INT32 bound
+    (K > 137438) -- and its count then meets the target on both blocks."""
     M, N = 128, 128
     A = oz.generate_matrix(M, K, phi=phi, seed=51)
     B = oz.generate_matrix(K, N, phi=phi, seed=52)
@@ -128,10 +127,13 @@ def test_autotune_scheme_choice(executor, K, phi, target):
     if K > 137438:
         assert scheme == 1
         return
-    # Scheme II at 20 moduli on the same two blocks decides which scheme is due
-    C20 = _run(executor, 2, A, B, 20)
-    e20 = max(oz.block_error(executor, dA, dB, _dev(C20), M, N, K, block=64, seed=sd) for sd in (3, 3 ^ 0x5bd1e995))
-    if e20 > target:
+    # Scheme II on the same two blocks decides which scheme is due
+    def e2(S2):
+        C2 = _run(executor, 2, A, B, S2)
+        return max(oz.block_error(executor, dA, dB, _dev(C2), M, N, K, block=64, seed=sd)
+                   for sd in (3, 3 ^ 0x5bd1e995))
+    if e2(20) > target:
         assert scheme == 1
-    else:
-        assert scheme == 2 or S * (S + 1) // 2 < 20
+    elif e2(19) <= target:   # Scheme II below its cap: taken unless Scheme I is cheaper
+        assert scheme == 2 or S * (S + 1) // 2 < 19
+    # else Scheme II only at its cap, where the knob checks more blocks: either scheme
