@@ -544,6 +544,18 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
             return gemm_overlapped(ws, A, B, C, chunks);
         }
     }
+    // Untimed calls with the default configuration run B's statistics and
+    // slicer on a second stream beside A's: the HBM-bound statistics of one
+    // operand overlap the issue-bound slicer of the other.  The GEMM waits
+    // for both.  Calls with timings keep the four steps in order.
+    const bool dual = !timings && K && ws->cfg.overlap_chunks == 0;
+    cudaStream_t sb = st;
+    if (dual) {
+        OZA_CUDA_TRY(overlap_init(ws), "oza_gemm: second stream");
+        sb = ws->ov.s_slice;
+        OZA_CUDA_TRY(cudaEventRecord(ws->ov.start, st), "CUDA: event record");
+        OZA_CUDA_TRY(cudaStreamWaitEvent(sb, ws->ov.start, 0), "CUDA: stream wait");
+    }
     if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[0], st), "CUDA: event record");
     if (K == 0) {
         // Empty inner dimension: the product is exactly zero.
@@ -553,15 +565,19 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         const int offset = ws->scheme == OZA_SCHEME2 ? ws->k_param : 0;
         // step 1
         OZA_CUDA_TRY(oza::launch_stats_rows(A, M, K, offset, ws->shiftA, ex->sms, st), "step1 rows");
-        OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, st), "step1 cols");
+        OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, sb), "step1 cols");
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[1], st), "CUDA: event record");
         // step 2
         OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A, M, K, ws->shiftA, ws->S, ws->beta, offset, ws->aplanes, ws->Mp,
                                             ws->Kp, ex->sms, st),
                      "step2 rows");
         OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
-                                            ws->bplanes, ws->Np, ws->Kp, st),
+                                            ws->bplanes, ws->Np, ws->Kp, sb),
                      "step2 cols");
+        if (dual) {
+            OZA_CUDA_TRY(cudaEventRecord(ws->ov.end, sb), "CUDA: event record");
+            OZA_CUDA_TRY(cudaStreamWaitEvent(st, ws->ov.end, 0), "CUDA: stream wait");
+        }
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[2], st), "CUDA: event record");
         // step 3
         oza::GemmPlan plan;
