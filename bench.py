@@ -102,9 +102,11 @@ def workload(args):
          "l2": f"inputs ({(M * K + K * N) * 8 / 2**30:.2f} GiB) "
                + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
                   "fit in L2: timings include L2 reuse")}
-    # non-default step-3 settings are part of the workload's description
+    # non-default settings are part of the workload's description
     if getattr(args, "overlap_chunks", 0):
         w["overlap_chunks"] = args.overlap_chunks
+    else:
+        w["steps_1_2"] = "A's and B's statistics and slicers on two streams (untimed calls; steps_ms: in order)"
     return w
 
 
