@@ -741,8 +741,8 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
 //   warp 0      TMA producer (4-stage ring of A 128x128 + B^T 256x128 int8 tiles)
 //   warp 1      TMEM allocation, UMMA issue (one elected lane)
 //   warps 2..   epilogue, EW warps; warp w reads TMEM lanes 32 (w % 4).. (its
-//               lane quadrant): with EW = 4 all 256 columns in two halves, with
-//               EW = 8 the column half (w - 2) / 4.  Four warps measured 1-2%
+//               lane quadrant): with EW = 4 all the tile's columns, with EW = 8
+//               the column half (w - 2) / 4.  Four warps measured 1-2%
 //               faster at large K (the epilogue hides behind a unit's MMAs);
 //               units of few k-blocks, where the epilogue is the longer side,
 //               take eight.
@@ -758,8 +758,10 @@ constexpr int kEpi8Below = 8;
 constexpr int kStages = 4;
 constexpr int kABytes = kTileM * kTileK;   // 16 KB per stage
 constexpr int kBBytes = kTileN * kTileK;   // 32 KB per stage
-constexpr uint32_t kAccCols = kTileN;      // TMEM columns per accumulator
+constexpr uint32_t kAccCols = 256;         // TMEM column stride between the two accumulators
 constexpr uint32_t kTmemCols = 2 * kAccCols;
+constexpr int kEpiChunks = kTileN / 32;    // 32-column TMEM loads per tile row
+static_assert(kTileN % 32 == 0 && kTileN <= (int)kAccCols, "tile width: a multiple of 32, at most 256");
 constexpr int kGemmSmem = kStages * (kABytes + kBBytes) + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int kEpiI32 = 0;
 constexpr int kEpiCoef = 1;
@@ -788,16 +790,15 @@ __device__ __forceinline__ void tile_coords(int t, const GemmArgs& a, int& mt, i
     mt = a.mt0 + b * a.band + (tb - nt * rows);
 }
 
-// One work unit's epilogue for one warp: 32 TMEM lanes (rows) x 128 columns
-// (`half` of the 256-column accumulator at taddr) of output tile column nt.
+// One work unit's epilogue for one warp: 32 TMEM lanes (rows) x the 32-column
+// chunks [c0, c1) of the accumulator at taddr, of output tile column nt.
 template <int EPI>
 __device__ __forceinline__ void epilogue_unit(int32_t* ctc, uint8_t* coef, long long Mp, long long Np, int S,
-                                              uint32_t taddr, long long row, int grp, int nt, int half) {
+                                              uint32_t taddr, long long row, int grp, int nt, int c0, int c1) {
     if (EPI == kEpiI32) {
-        int32_t* dst = ctc + (size_t)grp * Mp * Np + (size_t)row * Np +
-                       (size_t)nt * kTileN + half * (kTileN / 2);
+        int32_t* dst = ctc + (size_t)grp * Mp * Np + (size_t)row * Np + (size_t)nt * kTileN;
 #pragma unroll 1
-        for (int c = 0; c < kTileN / 64; ++c) {
+        for (int c = c0; c < c1; ++c) {
             uint32_t r[32];
             tmem_ld32(taddr + c * 32, r);
             tmem_ld_wait();
@@ -811,10 +812,9 @@ __device__ __forceinline__ void epilogue_unit(int32_t* ctc, uint8_t* coef, long 
         // coefficient ((C mod m_g) * inv_g) mod m_g, one byte.
         const ModConst mc = c_mod[grp];
         const uint32_t inv = c_crt[S - 1].inv[grp], c16 = c_crt[S - 1].c16inv[grp];
-        uint8_t* dst = coef + (size_t)grp * Mp * Np + (size_t)row * Np +
-                       (size_t)nt * kTileN + half * (kTileN / 2);
+        uint8_t* dst = coef + (size_t)grp * Mp * Np + (size_t)row * Np + (size_t)nt * kTileN;
 #pragma unroll 1
-        for (int c = 0; c < kTileN / 64; ++c) {
+        for (int c = c0; c < c1; ++c) {
             uint32_t r[32];
             tmem_ld32(taddr + c * 32, r);
             tmem_ld_wait();
@@ -1057,7 +1057,10 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3;                 // TMEM lane quadrant this warp may access
-        const int h0 = EW == 8 ? (warp - 2) >> 2 : 0, h1 = EW == 8 ? h0 + 1 : 2;   // column halves
+        // 32-column chunks of this warp: all of them (4 warps) or one half (8 warps)
+        const int half = (warp - 2) >> 2;
+        const int c0 = EW == 8 ? half * ((kEpiChunks + 1) / 2) : 0;
+        const int c1 = EW == 8 ? (half ? kEpiChunks : (kEpiChunks + 1) / 2) : kEpiChunks;
         const int row_local = q * 32 + lane;
         int local = 0;
         bool ok = true;
@@ -1074,11 +1077,8 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
                 continue;
             }
             tc_fence_after();
-            for (int half = h0; half < h1; ++half) {
-                const uint32_t taddr =
-                    tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols + (uint32_t)(half * (kTileN / 2));
-                epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, half);
-            }
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols;
+            epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, c0, c1);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[acc]);
