@@ -2,9 +2,9 @@
 // Mirrors include/ozablas/core/workspace.hpp:14-103 of IlyaNyrkov/ozablas.
 //
 // Layout note: by default the device buffers are laid out for the sm_100a
-// kernels, not as in the reference.  Slices/residues are K-major and zero
-// padded: get_A_slices() is int8 [S][Mp][Kp], get_B_slices() is int8
-// [S][Np][Kp] (B transposed), get_C_tc() is int32 [S][Mp][Np] with plane g
+// kernels, not as in the reference.  Slices/residues are K-major and padded
+// (zeros in the K padding; rows past M and N unwritten): get_A_slices() is
+// int8 [S][Mp][Kp], get_B_slices() is int8 [S][Np][Kp] (B transposed), get_C_tc() is int32 [S][Mp][Np] with plane g
 // holding group g (Scheme II: residue g; Scheme I: slice-sum group g+2), and
 // null for Scheme II, whose INT32 products never reach memory.  The padded
 // extents are get_Mp()/get_Np()/get_Kp().  Constructed with

@@ -518,24 +518,21 @@ __device__ __forceinline__ void slice_rows_chunk(const double* __restrict__ A, l
                                                  long long r, long long ch) {
     constexpr int E = SCHEME == 2 ? 8 : 16;
     const long long c0 = ch * E;
+    // Rows past `rows` (tile padding) are not written: the products they feed
+    // land in rows of the INT32 / coefficient planes that no later step reads.
+    // The K padding of real rows is written as zeros.
+    if (r >= rows) return;
     double v[E];
-    int sh = 0;
-    if (r < rows) {
-        sh = shift[r];
-        const double* src = A + r * cols + c0;
+    const int sh = shift[r];
+    const double* src = A + r * cols + c0;
 #pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
-    } else {
-#pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = 0.0;
-    }
+    for (int i = 0; i < E; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
     int8_t* dst = out + (size_t)r * cols_p + c0;
     if (store_if_zero<E>(v, SCHEME == 2 ? SC : S, dst, plane)) return;
     if (SCHEME == 2) {
         residuesE<SC, WIDE, E>(v, sh, pow2_or_zero(sh), dst, plane);
     } else {
-        slices16(reinterpret_cast<const double(&)[16]>(v), r < rows ? -sh : -1023, beta, S,
-                 reinterpret_cast<uint4*>(dst), plane);
+        slices16(reinterpret_cast<const double(&)[16]>(v), -sh, beta, S, reinterpret_cast<uint4*>(dst), plane);
     }
 }
 
@@ -546,7 +543,7 @@ __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_rows(
     constexpr int E = SCHEME == 2 ? 8 : 16;
     const size_t plane = (size_t)plane_rows * (size_t)cols_p;
     for (GridWalk w((long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, cols_p / E);
-         w.r < rows_p; w.next())
+         w.r < rows; w.next())
         slice_rows_chunk<SCHEME, SC, WIDE>(A, rows, cols, shift, S, beta, out, cols_p, plane, w.r, w.c);
 }
 
@@ -562,6 +559,9 @@ __device__ __forceinline__ void slice_cols_tile(const double* __restrict__ B, lo
     __shared__ double tile[128][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long n0 = bx * 32, k0 = by * 128;
+    // Rows of B^T past N (tile padding) are not written: their products land in
+    // columns of the INT32 / coefficient planes that no later step reads.
+    if (n0 >= N) return;   // block-uniform
     // Load: warp w reads rows k0 + w + 8 i, 32 consecutive columns.
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
@@ -571,9 +571,10 @@ __device__ __forceinline__ void slice_cols_tile(const double* __restrict__ B, lo
     __syncthreads();
     const long long n = n0 + lane;
     const int kg = warp;   // 16-row group
-    int e = (n < N) ? max_exp_from_bits(colmax[n]) : -1023;
-    int sh = offset - e;
-    if (by == 0 && kg == 0 && n < N) shift[n] = sh;
+    if (n >= N) return;   // no barrier follows
+    const int e = max_exp_from_bits(colmax[n]);
+    const int sh = offset - e;
+    if (by == 0 && kg == 0) shift[n] = sh;
     double v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = tile[kg * 16 + i][lane];
@@ -1352,7 +1353,7 @@ __global__ void __launch_bounds__(256, 3) k_group_slice_rows(const GroupProblemD
                                                              const __grid_constant__ GroupLaunchDev L) {
     const int q = group_find(L, blockIdx.x);
     const GroupProblemDev& P = probs[L.ids[q]];
-    const long long total = P.Mp * (P.Kp / 8);
+    const long long total = P.M * (P.Kp / 8);   // real rows only (see slice_rows_chunk)
     const long long base = (blockIdx.x - L.start[q]) * (256 * kGroupRowChunks) + threadIdx.x;
 #pragma unroll 1
     for (int r = 0; r < kGroupRowChunks; ++r) {
@@ -1371,7 +1372,7 @@ __global__ void __launch_bounds__(256, 3) k_group_slice_cols(const GroupProblemD
     const int q = group_find(L, blockIdx.x);
     const GroupProblemDev& P = probs[L.ids[q]];
     const long long t = blockIdx.x - L.start[q];
-    const long long nx = P.Np / 32, ny = P.Kp / 128;
+    const long long nx = (P.N + 31) / 32, ny = P.Kp / 128;   // real columns only (see slice_cols_tile)
 #pragma unroll 1
     for (int r = 0; r < kGroupColTiles; ++r) {
         const long long by = (t / nx) * kGroupColTiles + r;
@@ -1516,7 +1517,7 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift, int S,
                               int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
                               cudaStream_t st, size_t plane_rows) {
-    long long chunks = (long long)rows_p * (long long)(cols_p / (scheme == 2 ? 8 : 16));
+    long long chunks = (long long)rows * (long long)(cols_p / (scheme == 2 ? 8 : 16));
     if (chunks == 0) return cudaSuccess;
     const int grid = grid_for(chunks, 256, sms);
     const long long R = (long long)rows, C = (long long)cols, RP = (long long)rows_p, CP = (long long)cols_p;
@@ -1543,8 +1544,9 @@ cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t c
 cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
                               int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
                               cudaStream_t st) {
-    if (Np == 0 || Kp == 0) return cudaSuccess;
-    const dim3 grid((unsigned)(Np / 32), (unsigned)(Kp / 128));
+    if (N == 0 || Kp == 0) return cudaSuccess;
+    if (N > Np) return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)((N + 31) / 32), (unsigned)(Kp / 128));
     const long long KK = (long long)K, NN = (long long)N, NP = (long long)Np, KP = (long long)Kp;
     if (scheme == 1) {
         k_slice_cols<1, 0, false><<<grid, 256, 0, st>>>(B, KK, NN, colmax, offset, S, beta, shift, out, NP, KP);
@@ -1782,8 +1784,8 @@ cudaError_t group_plan_build(const GroupProblem* in, int count, int* err, GroupP
         switch (stage) {
             case 0: return (d.M + 7) / 8;
             case 1: return ((d.N + 63) / 64) * ((d.K + 255) / 256);
-            case 2: return (d.Mp * (d.Kp / 8) + 256 * kGroupRowChunks - 1) / (256 * kGroupRowChunks);
-            case 3: return (d.Np / 32) * ((d.Kp / 128 + kGroupColTiles - 1) / kGroupColTiles);
+            case 2: return (d.M * (d.Kp / 8) + 256 * kGroupRowChunks - 1) / (256 * kGroupRowChunks);
+            case 3: return ((d.N + 31) / 32) * ((d.Kp / 128 + kGroupColTiles - 1) / kGroupColTiles);
             default: return (d.M * ((d.N + 3) / 4) + 255) / 256;
         }
     };

@@ -26,10 +26,13 @@ def _check_all(got, ref):
 
 
 def _padding_zero(got):
+    """The K padding of every real row of the A and B^T planes is zero (it
+    enters the sums); rows past M and N are left unwritten, since the products
+    they feed are never read."""
     i = got["ws"].info
     M, N, K = i["M"], i["N"], i["K"]
-    assert not got["A_planes"][:, M:, :].any() and not got["A_planes"][:, :, K:].any()
-    assert not got["B_planes"][:, N:, :].any() and not got["B_planes"][:, :, K:].any()
+    assert not got["A_planes"][:, :M, K:].any()
+    assert not got["B_planes"][:, :N, K:].any()
 
 
 @pytest.mark.parametrize("S", [1, 2, 4, 7, 8, 9, 12, 16, 18, 20])
