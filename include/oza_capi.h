@@ -182,7 +182,8 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
 /* ---- GEMM tuning ------------------------------------------------------------ */
 /* Step-3 kernel configuration of a workspace (0 fields: library defaults).
  *   band         m-tiles (128 rows each) per rasterisation band of the GEMM's
- *                output tiles (default 16)
+ *                output tiles (default: Scheme II the m-tiles of 32 MiB of one
+ *                A plane, at least 16; Scheme I 16)
  *   wait_hint_ns suspend-time hint of the kernel's mbarrier waits (0: poll)
  *   overlap_chunks  Scheme II fused path, calls without timings: >= 2 splits
  *                the GEMM into that many row chunks and overlaps A's slicing

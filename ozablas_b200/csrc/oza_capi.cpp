@@ -661,7 +661,7 @@ oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, do
     if (!ws || !best) return fail(OZA_INVALID_ARG, "oza_autotune_gemm: null argument");
     const oza_gemm_config_t saved = ws->cfg;
     std::vector<oza_gemm_config_t> cand;
-    const int bands[] = {8, 16, 32};
+    const int bands[] = {0, 8, 16, 32};   // 0: the library's default for the shape
     for (int b : bands) cand.push_back(oza_gemm_config_t{b, saved.wait_hint_ns, saved.overlap_chunks});
     float best_t = 1e30f;
     oza_gemm_config_t best_c = saved;

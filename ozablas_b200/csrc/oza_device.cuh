@@ -23,7 +23,7 @@ enum DeviceError : int {
 //   c21/42/63 = 2^21, 2^42, 2^63 mod m, symmetric representatives
 //   inv    = (M/m)^-1 mod m for the current slice count (per table row)
 //   dig[w] = bytes 4w..4w+3 of (256^i mod m, symmetric, int8), i = 0..15
-//   magic32 = ceil(2^32 / m): floor(u / m) == umulhi(u, magic32) for u < 2^32 / m
+//   magic32 = ceil(2^32 / m): u mod m == umulhi(u * magic32 mod 2^32, m) for u < 2^32 / m
 //   bh = m * 2^10 + (m-1)/2, adj = 256 - (m-1)/2 (residue reduction of the MMA slicer)
 struct ModConst {
     uint32_t m;
@@ -47,15 +47,15 @@ struct CrtTable {
     uint32_t P[kMaxSlices][5];  // M / m_i
     uint32_t inv[kMaxSlices];   // (M / m_i)^-1 mod m_i
     uint32_t c16inv[kMaxSlices];  // (2^16 * inv_i) mod m_i
-    unsigned long long recip48[kMaxSlices];   // floor(2^48 / m_i), for the quotient estimate
+    double rinv[kMaxSlices];      // 1 / m_i rounded to double, for the quotient estimate
     // Triples (3t, 3t+1, 3t+2), t < S / 3
     uint32_t TP[kMaxSlices / 3][5];           // M / (m_a m_b m_c)
     uint32_t tk[kMaxSlices / 3];              // (m_b m_c) | (m_a m_c) << 16: dp2a weights of c_a, c_b
     uint32_t tab[kMaxSlices / 3];             // m_a m_b: weight of c_c
-    unsigned long long trecip48[kMaxSlices / 3];  // floor(2^48 / (m_a m_b m_c))
+    double trinv[kMaxSlices / 3];             // 1 / (m_a m_b m_c) rounded to double
     // The last two residues (S - 2, S - 1) when S mod 3 == 2
     uint32_t DP[5];                           // M / (m_{S-2} m_{S-1})
-    unsigned long long drecip48;              // floor(2^48 / (m_{S-2} m_{S-1}))
+    double drinv;                             // 1 / (m_{S-2} m_{S-1}) rounded to double
     int nlimbs;                   // limbs of M that can be nonzero
 };
 

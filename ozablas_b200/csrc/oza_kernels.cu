@@ -141,7 +141,7 @@ cudaError_t upload_tables() {
                 for (int l = 0; l < 5; ++l) t.P[i][l] = 0;
                 t.inv[i] = 0;
                 t.c16inv[i] = 0;
-                t.recip48[i] = 0;
+                t.rinv[i] = 0.0;
                 continue;
             }
             cofactor({i}, t.P[i]);
@@ -155,25 +155,25 @@ cudaError_t upload_tables() {
                 }
             t.inv[i] = inv;
             t.c16inv[i] = (uint32_t)((65536ull * inv) % m);
-            t.recip48[i] = (1ull << 48) / m;
+            t.rinv[i] = 1.0 / (double)m;
         }
         for (int q = 0; q < kMaxSlices / 3; ++q) {
             const int a = 3 * q, b = a + 1, c = a + 2;
             for (int l = 0; l < 5; ++l) t.TP[q][l] = 0;
             t.tk[q] = t.tab[q] = 0;
-            t.trecip48[q] = 0;
+            t.trinv[q] = 0.0;
             if (c >= S) continue;
             const uint64_t ma = kModuli[a], mb = kModuli[b], mc = kModuli[c];
             cofactor({a, b, c}, t.TP[q]);
             t.tk[q] = (uint32_t)(mb * mc) | ((uint32_t)(ma * mc) << 16);
             t.tab[q] = (uint32_t)(ma * mb);
-            t.trecip48[q] = (1ull << 48) / (ma * mb * mc);
+            t.trinv[q] = 1.0 / (double)(ma * mb * mc);
         }
         for (int l = 0; l < 5; ++l) t.DP[l] = 0;
-        t.drecip48 = 0;
+        t.drinv = 0.0;
         if (S % 3 == 2) {
             cofactor({S - 2, S - 1}, t.DP);
-            t.drecip48 = (1ull << 48) / ((uint64_t)kModuli[S - 2] * kModuli[S - 1]);
+            t.drinv = 1.0 / (double)((uint64_t)kModuli[S - 2] * kModuli[S - 1]);
         }
     }
     e = cudaMemcpyToSymbol(c_mod, mc, sizeof(mc));
@@ -381,6 +381,13 @@ __device__ __forceinline__ int symmetric_residue(int s, int d0, int d1, int d2, 
     return (int)r - ((r > (mc.m >> 1)) ? (int)mc.m : 0);
 }
 
+// (a * b) / 2^32 + c in one multiply (PTX mad.hi).
+__device__ __forceinline__ uint32_t mulhi_add(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
     return (uint32_t)(a & 0xFF) | ((uint32_t)(b & 0xFF) << 8) | ((uint32_t)(c & 0xFF) << 16) |
            ((uint32_t)(d & 0xFF) << 24);
@@ -404,8 +411,11 @@ __device__ __forceinline__ int cvt_s8(double v) {
 // NARROW (K_param <= 62, so |x| <= 2^62): x = sum_{i<8} d_i 256^i with signed
 // byte digits d_i = byte_i(x + 0x8080...80) - 128, and
 //   u = m 2^10 + (m-1)/2 + sum_i d_i (256^i mod m)       (two dp4a)
-// lies in (0, 2^19); q = umulhi(u, ceil(2^32/m)) = floor(u/m) exactly (u m <
-// 2^32) and the low byte of u - q m + 256 - (m-1)/2 is the symmetric residue.
+// lies in (0, 2^19).  With c = ceil(2^32/m) = (2^32 + e)/m, 0 <= e < m, the low
+// word f = u c mod 2^32 equals (u mod m) 2^32/m + u e/m (as u e < 2^32), so
+// floor(f m / 2^32) = u mod m exactly: one multiply for f and one mad.hi that
+// also adds 256 - (m-1)/2, whose low byte is the symmetric residue (Lemire,
+// Kaser and Kurz, "Faster remainder by direct computation", 2019).
 // WIDE (|x| < 2^84): radix-2^21 digits and the magic division of
 // symmetric_residue.
 template <int S, bool WIDE, int E>
@@ -427,7 +437,7 @@ __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p
 #pragma unroll
             for (int i = 0; i < E; ++i) {
                 const uint32_t u = (uint32_t)__dp4a(dhi[i], (int)mc.dig[1], __dp4a(dlo[i], (int)mc.dig[0], mc.bh));
-                r[i] = u - __umulhi(u, mc.magic32) * mc.m + (uint32_t)mc.adj;
+                r[i] = mulhi_add(u * mc.magic32, mc.m, (uint32_t)mc.adj);
             }
             uint32_t wds[E / 4];
 #pragma unroll
@@ -613,25 +623,31 @@ __device__ __forceinline__ uint32_t crt_coeff(int32_t C, uint32_t m, uint32_t ma
 
 // Running state of one element: T = sum c_s * (M / m_s) as NL 64-bit column
 // sums of 32-bit limb products (each product below 2^58, at most 20 of them),
-// and a fixed-point estimate of T / M in units of 2^-48 (an underestimate by
-// less than 2^-18).
+// and an FP64 estimate of T / M: the sum of d / P over the terms d * (M / P)
+// added, each d converted exactly (d < 2^32) and multiplied by 1 / P rounded
+// to double.  T / M < S <= 20, so each of the at most 20 fused multiply-adds
+// rounds by at most 2^-49, and the reciprocals' relative error of 2^-53 adds
+// at most 20 * 2^-53: the estimate is within 2^-44 of T / M.  It runs on the
+// FP64 pipe, beside the integer multiplies of the limbs.
 template <int NL>
 struct CrtAcc {
     unsigned long long a[NL];
-    unsigned long long q;
+    double q;
     __device__ __forceinline__ void zero() {
 #pragma unroll
         for (int l = 0; l < NL; ++l) a[l] = 0ull;
-        q = 0ull;
+        q = 0.0;
     }
-    // d * W where W = M / (product of the moduli d stands for), recip = floor(2^48 / that product)
-    __device__ __forceinline__ void add(const uint32_t (&W)[5], unsigned long long recip, uint32_t d) {
+    // d * W where W = M / P for the product P of the moduli d stands for, rinv = 1 / P
+    __device__ __forceinline__ void add(const uint32_t (&W)[5], double rinv, uint32_t d) {
 #pragma unroll
         for (int l = 0; l < NL; ++l) a[l] += (unsigned long long)d * W[l];
-        q += (unsigned long long)d * recip;
+        // 2^52 + d exactly, minus 2^52: d as a double without a conversion instruction
+        const double dd = __hiloint2double(0x43300000, (int)d) - 0x1p52;
+        q = fma(dd, rinv, q);
     }
     // one residue s with coefficient c < m_s
-    __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) { add(T.P[s], T.recip48[s], c); }
+    __device__ __forceinline__ void add(const CrtTable& T, int s, uint32_t c) { add(T.P[s], T.rinv[s], c); }
 };
 
 // r = x - y over N 32-bit limbs.  The whole borrow chain is one asm block: the
@@ -682,9 +698,10 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
         carry = v >> 32;
     }
     t[NL] = (uint32_t)carry;
-    // nearest quotient: the estimate is q* or q* - 1, so V = T - q M is either
+    // nearest quotient: with the estimate within 2^-44 of T / M,
+    // floor(estimate + 1/2 - 2^-40) is q* or q* - 1, so V = T - q M is either
     // the answer or the answer + M (then V >= floor(M/2)).
-    const uint32_t q = (uint32_t)((acc.q + (1ull << 47)) >> 48);
+    const uint32_t q = __double2uint_rz(acc.q + (0.5 - 0x1p-40));
     uint32_t qm[L];
     {
         unsigned long long c = 0;
@@ -1147,17 +1164,17 @@ __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef,
         const uint32_t d1 = __dp2a_hi(k, x01, __byte_perm(wc, 0, 0x4441) * kab);
         const uint32_t d2 = __dp2a_lo(k, x23, __byte_perm(wc, 0, 0x4442) * kab);
         const uint32_t d3 = __dp2a_hi(k, x23, __byte_perm(wc, 0, 0x4443) * kab);
-        st[0].add(T.TP[t], T.trecip48[t], d0);
-        st[1].add(T.TP[t], T.trecip48[t], d1);
-        st[2].add(T.TP[t], T.trecip48[t], d2);
-        st[3].add(T.TP[t], T.trecip48[t], d3);
+        st[0].add(T.TP[t], T.trinv[t], d0);
+        st[1].add(T.TP[t], T.trinv[t], d1);
+        st[2].add(T.TP[t], T.trinv[t], d2);
+        st[3].add(T.TP[t], T.trinv[t], d3);
     }
     if constexpr (S % 3 == 2) {
         const uint32_t ma = c_mod[S - 2].m, mb = c_mod[S - 1].m;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const uint32_t d = ((w[S - 2] >> (8 * e)) & 0xFFu) * mb + ((w[S - 1] >> (8 * e)) & 0xFFu) * ma;
-            st[e].add(T.DP, T.drecip48, d);
+            st[e].add(T.DP, T.drinv, d);
         }
     } else if constexpr (S % 3 == 1) {
 #pragma unroll
@@ -1594,8 +1611,20 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.n_tiles = (int)(p.Np / kTileN);
     a.k_blocks = (int)(p.Kp / kTileK);
     a.total_tiles = a.m_tiles * a.n_tiles;
-    // Default band: 16 m-tiles (2048 rows of A) per rasterisation band.
-    const int band = p.band > 0 ? p.band : 16;
+    // Default band.  Scheme II: the m-tiles of 32 MiB of one A plane, at
+    // least 16 (K = 8192: 32 m-tiles, 4096 rows).  The band of A stays in L2
+    // while B's plane streams past once per band: at 8192^3, S = 16, bands of
+    // 32 read 3.2 GB per launch against 5.3 GB for 16 (64: 10.9 GB), 1-2%
+    // faster; at 16384 x 16384 x 1024 the whole M (128 m-tiles) is 2.4% faster
+    // than 16.  Scheme I units read all slice pairs of a tile: 16 m-tiles.
+    int band = p.band;
+    if (band <= 0) {
+        band = 16;
+        if (p.coef) {
+            const long long fit = (32ll << 20) / ((long long)kTileM * (long long)p.Kp);
+            if (fit > band) band = (int)(fit < a.m_tiles ? fit : a.m_tiles);
+        }
+    }
     a.band = a.m_tiles < band ? a.m_tiles : band;
     a.groups = p.pairs.num_groups;
     a.Mp = (long long)p.Mp;
