@@ -67,17 +67,18 @@ def parse():
     return p.parse_args()
 
 
-def launches_per_call(M, scheme, materialize, overlap_chunks=0):
+def launches_per_call(M, N, K, scheme, materialize, overlap_chunks=0):
     """Kernels one device-buffer GEMM call launches (Scheme II/I, K > 0): the
     four steps in order are 6 launches (row and column statistics, the two
     slicers, the GEMM, the reconstruction).  The Scheme II fused path with
     overlapped stages launches B's statistics and slicer once and, per row
     chunk, A's statistics, A's slicer, a GEMM and a CRT.  The chunk rule is the
-    library's (oza_gemm): by default 2 chunks for 8..47 row tiles of 128, else
-    1; a requested count c becomes ceil(tiles / q) chunks of q = ceil(tiles /
-    min(c, 16, tiles)) tiles."""
+    library's (oza_gemm): by default 2 chunks for 8..47 row tiles of 128 when
+    2 M N K >= 2^33, else 1; a requested count c becomes ceil(tiles / q) chunks
+    of q = ceil(tiles / min(c, 16, tiles)) tiles."""
     tiles = (M + 127) // 128
-    chunks = overlap_chunks if overlap_chunks else (2 if 8 <= tiles < 48 else 1)
+    big = 2.0 * M * N * K >= 2.0 ** 33
+    chunks = overlap_chunks if overlap_chunks else (2 if 8 <= tiles < 48 and big else 1)
     if chunks > 1:
         q = -(-tiles // min(chunks, 16, tiles))
         chunks = -(-tiles // q)
@@ -446,7 +447,7 @@ def run_ours(args, ws, rank, local):
                else load_traffic().get(workload(args)["workload"] + f"_S{S}"))
     bytes_h2d = (M * K + K * N) * 8
     bytes_d2h = M * N * 8
-    steps_kernels = launches_per_call(M, args.scheme, args.materialize, args.overlap_chunks)
+    steps_kernels = launches_per_call(M, N, K, args.scheme, args.materialize, args.overlap_chunks)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

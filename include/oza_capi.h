@@ -189,8 +189,9 @@ oza_status_t oza_selftest_wait_timeout(oza_exec_t ex, double limit_s, int* code,
  *                the GEMM into that many row chunks and overlaps A's slicing
  *                and each chunk's reconstruction with the GEMM on two more
  *                streams; 1: the steps in order; 0: 2 chunks for 8 to 47 row
- *                tiles of 128, else 1.  Calls with timings run the steps in
- *                order.
+ *                tiles of 128 when 2 M N K >= 2^33, else 1 (and B's steps 1-2
+ *                on a second stream when M K + K N >= 2^26).  Calls with
+ *                timings run the steps in order.
  * Results do not depend on the configuration (bit-identical).
  * Extension: the reference's step 3 is cuBLAS with its own heuristics. */
 typedef struct {

@@ -163,18 +163,23 @@ void overlap_release(oza_workspace* ws) {
     if (o.s_crt) cudaStreamDestroy(o.s_crt);
 }
 
-cudaError_t overlap_init(oza_workspace* ws) {
+// The second stream and its two events (the two-stream steps 1-2), and with
+// `chunks` > 0 the reconstruction stream and the events of that many row
+// chunks: each object made on first use and kept with the workspace.
+cudaError_t overlap_init(oza_workspace* ws, int chunks) {
     auto& o = ws->ov;
-    if (o.end) return cudaSuccess;
-    cudaError_t e = cudaStreamCreateWithFlags(&o.s_slice, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&o.s_crt, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.start, cudaEventDisableTiming);
-    for (int i = 0; i < oza_workspace::Overlap::kMaxChunks && e == cudaSuccess; ++i) {
-        e = cudaEventCreateWithFlags(&o.a_done[i], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.g_done[i], cudaEventDisableTiming);
+    cudaError_t e = cudaSuccess;
+    if (!o.s_slice) e = cudaStreamCreateWithFlags(&o.s_slice, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !o.start) e = cudaEventCreateWithFlags(&o.start, cudaEventDisableTiming);
+    if (e == cudaSuccess && !o.end) e = cudaEventCreateWithFlags(&o.end, cudaEventDisableTiming);
+    if (chunks > 0) {
+        if (e == cudaSuccess && !o.s_crt) e = cudaStreamCreateWithFlags(&o.s_crt, cudaStreamNonBlocking);
+        const int n = std::min(chunks, (int)oza_workspace::Overlap::kMaxChunks);
+        for (int i = 0; i < n && e == cudaSuccess; ++i) {
+            if (!o.a_done[i]) e = cudaEventCreateWithFlags(&o.a_done[i], cudaEventDisableTiming);
+            if (e == cudaSuccess && !o.g_done[i]) e = cudaEventCreateWithFlags(&o.g_done[i], cudaEventDisableTiming);
+        }
     }
-    // `end` last: its presence marks a complete set-up.
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o.end, cudaEventDisableTiming);
     return e;
 }
 
@@ -533,25 +538,32 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         // at 4096^3 over the steps in order.  From 48 tiles the GEMM dominates
         // and a single full launch is faster per clock than chunk launches
         // sharing the SMs with the slicer: at 8192^3 the steps in order run at
-        // 132.5 TFLOP/s against 127-129 with 2 to 4 chunks.
+        // 132.5 TFLOP/s against 127-129 with 2 to 4 chunks.  Below 2^33 FP64
+        // flops (2 M N K) the extra streams' synchronisation costs more than
+        // the overlap gains: the steps in order.
         int chunks = ws->cfg.overlap_chunks;
         if (chunks == 0) {
             const size_t tiles = (M + oza::kTileM - 1) / oza::kTileM;
-            chunks = (tiles >= 8 && tiles < 48) ? 2 : 1;
+            const double flops = 2.0 * (double)M * (double)N * (double)K;
+            chunks = (tiles >= 8 && tiles < 48 && flops >= 0x1p33) ? 2 : 1;
         }
         if (chunks >= 2) {
-            OZA_CUDA_TRY(overlap_init(ws), "oza_gemm: overlap streams");
+            OZA_CUDA_TRY(overlap_init(ws, chunks), "oza_gemm: overlap streams");
             return gemm_overlapped(ws, A, B, C, chunks);
         }
     }
     // Untimed calls with the default configuration run B's statistics and
     // slicer on a second stream beside A's: the HBM-bound statistics of one
     // operand overlap the issue-bound slicer of the other.  The GEMM waits
-    // for both.  Calls with timings keep the four steps in order.
-    const bool dual = !timings && K && ws->cfg.overlap_chunks == 0;
+    // for both.  Only where steps 1-2 are long enough to pay for the second
+    // stream's synchronisation: M K + K N of at least 2^26 elements (8192^3:
+    // -2.1% per call); smaller calls, and calls with timings, keep the four
+    // steps in order.
+    const bool dual = !timings && K && ws->cfg.overlap_chunks == 0 &&
+                      (double)M * (double)K + (double)K * (double)N >= 0x1p26;
     cudaStream_t sb = st;
     if (dual) {
-        OZA_CUDA_TRY(overlap_init(ws), "oza_gemm: second stream");
+        OZA_CUDA_TRY(overlap_init(ws, 0), "oza_gemm: second stream");
         sb = ws->ov.s_slice;
         OZA_CUDA_TRY(cudaEventRecord(ws->ov.start, st), "CUDA: event record");
         OZA_CUDA_TRY(cudaStreamWaitEvent(sb, ws->ov.start, 0), "CUDA: stream wait");
