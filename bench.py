@@ -168,12 +168,17 @@ class ClockSampler:
         self.samples = []          # (sm_mhz, reasons bitmask, power W)
         self.max_mhz = None
         self.stop = threading.Event()
+        self.ready = threading.Event()   # the poller is running (or gave up)
         self.t = None
 
     def _poll(self):
-        import pynvml
-        h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
-        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        try:
+            import pynvml
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001
+            self.ready.set()
+            return
         while not self.stop.is_set():
             try:
                 sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
@@ -182,6 +187,7 @@ class ClockSampler:
                 self.samples.append((sm, rs, pw))
             except Exception:  # noqa: BLE001
                 pass
+            self.ready.set()
             self.stop.wait(0.01)
 
     def __enter__(self):
@@ -196,6 +202,10 @@ class ClockSampler:
                     pass
             self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
+            # the timed region starts once the poller runs; its first sample,
+            # taken before the region, is dropped
+            self.ready.wait(5.0)
+            self.samples.clear()
         except Exception:  # noqa: BLE001
             self.t = None
         return self
