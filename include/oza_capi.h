@@ -209,11 +209,12 @@ oza_status_t oza_autotune_gemm(oza_ws_t ws, const double* A, const double* B, do
                                float* best_step3_ms);
 
 /* C = A * B with A, B, C in HOST memory (row-major; pinned for overlap),
- * synchronous.  Scheme II (fused path): the copies are pipelined with the
- * compute in row chunks of A -- B is copied and sliced while A's chunks
- * arrive, each chunk is sliced, multiplied and reconstructed as it lands,
- * and its rows of C are copied back while the next chunk runs.  Other
- * workspaces copy in, compute, copy out.  Device staging for A, B and C is
+ * synchronous.  Scheme II (fused path) and Scheme I: the copies are
+ * pipelined with the compute in row chunks of A -- B is copied and sliced
+ * while A's chunks arrive, each chunk is sliced, multiplied and
+ * reconstructed as it lands, and its rows of C are copied back while the next
+ * chunk runs.  Materialised Scheme II and reference-layout workspaces copy
+ * in, compute, copy out.  Device staging for A, B and C is
  * allocated in the workspace on the first call.  timings->total_ms is the
  * device time from the first copy to the last; the step fields are 0.
  * Results are bit-identical to oza_gemm.

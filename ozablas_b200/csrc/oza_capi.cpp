@@ -714,8 +714,12 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
     const size_t M = ws->M, N = ws->N, K = ws->K;
     OZA_CUDA_TRY(cudaEventRecord(h.t0, st), "CUDA: event record");
 
-    if (!ws->fused || K == 0) {
-        // Scheme I, the materialised path and K = 0: copy in, compute, copy out.
+    // Scheme II fused and Scheme I (without the reference-layout copies) take
+    // the row-chunk pipeline.
+    const bool pipelined = K && (ws->fused || (ws->scheme == OZA_SCHEME1 && !ws->a_ref));
+    if (!pipelined) {
+        // The materialised Scheme II path, the reference layouts and K = 0:
+        // copy in, compute, copy out.
         if (K) {
             OZA_CUDA_TRY(cudaMemcpyAsync(h.dA, hA, M * K * sizeof(double), cudaMemcpyHostToDevice, st), "H2D A");
             OZA_CUDA_TRY(cudaMemcpyAsync(h.dB, hB, K * N * sizeof(double), cudaMemcpyHostToDevice, st), "H2D B");
@@ -728,15 +732,20 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         // each A chunk is sliced, multiplied against all of B (its m-tiles
         // only) and reconstructed, and its rows of C go back while the next
         // chunk is computed.  Copies in and out run on their own streams.
-        const int offset = ws->k_param;
+        const bool s2 = ws->scheme == OZA_SCHEME2;
+        const int offset = s2 ? ws->k_param : 0;
         const size_t tile_m = oza::kTileM;
         const int mt_all = (int)((M + tile_m - 1) / tile_m);
-        // 32 chunks: the exposed tail after the last A chunk lands (its
-        // GEMM, CRT and copy-out) is 1/32 of the compute and of C.  At
+        // Scheme II: 32 chunks.  The exposed tail after the last A chunk lands
+        // (its GEMM, CRT and copy-out) is 1/32 of the compute and of C.  At
         // 8192^3 a chunk's compute (~0.28 ms) still keeps pace with its copy
         // (~0.31 ms), and the call ends ~1 ms above the PCIe floor (1 GiB in
-        // with the copy-out of C running beside the second half).
-        const int R0 = std::min(mt_all, (int)oza_workspace::HostPipe::kMaxChunks);
+        // with the copy-out of C running beside the second half).  Scheme I:
+        // 8 chunks.  Its compute outlasts the copies, and each chunk's GEMM
+        // streams every slice plane of B once per group, so fewer, larger
+        // chunks.
+        const int max_chunks = s2 ? (int)oza_workspace::HostPipe::kMaxChunks : 8;
+        const int R0 = std::min(mt_all, max_chunks);
         const int q = (mt_all + R0 - 1) / R0;   // m-tiles per chunk
         const int R = (mt_all + q - 1) / q;
         OZA_CUDA_TRY(cudaStreamWaitEvent(h.cin, h.t0, 0), "CUDA: stream wait");
@@ -773,16 +782,22 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
             plan.pairs = ws->pairs;
             plan.err = ws->err;
             plan.sms = ex->sms;
-            plan.ctc = nullptr;
-            plan.coef = ws->coef;
+            plan.ctc = s2 ? nullptr : ws->ctc;
+            plan.coef = s2 ? ws->coef : nullptr;
             plan.m_tile_begin = c * q;
             plan.m_tile_count = std::min(q, mt_all - c * q);
             plan.band = ws->cfg.band;
             plan.wait_hint_ns = (uint32_t)ws->cfg.wait_hint_ns;
             OZA_CUDA_TRY(oza::launch_gemm_i8(plan, st), "step3 gemm");
-            OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->shiftA + r0,
-                                              ws->shiftB, h.dC + r0 * N, ex->sms, st),
-                         "step4 crt");
+            if (s2) {
+                OZA_CUDA_TRY(oza::launch_crt_coef(ws->coef + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S,
+                                                  ws->shiftA + r0, ws->shiftB, h.dC + r0 * N, ex->sms, st),
+                             "step4 crt");
+            } else {
+                OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->beta,
+                                                      ws->shiftA + r0, ws->shiftB, h.dC + r0 * N, ex->sms, st),
+                             "step4 sum");
+            }
             OZA_CUDA_TRY(cudaEventRecord(h.done[c], st), "CUDA: event record");
             OZA_CUDA_TRY(cudaStreamWaitEvent(h.cout, h.done[c], 0), "CUDA: stream wait");
             OZA_CUDA_TRY(cudaMemcpyAsync(hC + r0 * N, h.dC + r0 * N, rows * N * sizeof(double),

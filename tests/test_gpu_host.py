@@ -43,13 +43,30 @@ def test_host_gemm_matches_device_gemm(executor, M, N, K, S, pinned):
     assert t.total_ms > 0
 
 
-@pytest.mark.parametrize("scheme,materialize", [(1, False), (2, True)])
-def test_host_gemm_unpipelined_paths(executor, scheme, materialize):
+@pytest.mark.parametrize("M,N,K,S", [(300, 200, 500, 6), (1000, 700, 900, 8), (2304, 512, 300, 4), (1, 1, 1, 3),
+                                     (1500, 130, 257, 9)])
+def test_host_gemm_scheme1_pipeline(executor, M, N, K, S):
+    """Scheme I on the row-chunk pipeline (up to 8 chunks), pinned and not."""
+    import torch
+    A = oz.generate_matrix(M, K, 0.5, 8)
+    B = oz.generate_matrix(K, N, 0.5, 9)
+    want = _device_result(executor, 1, A, B, S)
+    W = oz.WorkspaceScheme1(executor, M, N, K, S)
+    C = np.full((M, N), np.nan)
+    oz.ozaki_gemm_host(W, A, B, C)
+    assert np.array_equal(C.view(np.int64), want.view(np.int64))
+    hC = torch.full((M, N), float("nan"), dtype=torch.float64).pin_memory()
+    oz.ozaki_gemm_host(W, torch.from_numpy(A).pin_memory(), torch.from_numpy(B).pin_memory(), hC)
+    assert np.array_equal(hC.numpy().view(np.int64), want.view(np.int64))
+
+
+def test_host_gemm_unpipelined_path(executor):
+    """Materialised Scheme II: copy in, compute, copy out."""
     M, N, K, S = 300, 200, 500, 6
     A = oz.generate_matrix(M, K, 0.5, 8)
     B = oz.generate_matrix(K, N, 0.5, 9)
-    want = _device_result(executor, scheme, A, B, S, materialize)
-    W = (oz.WorkspaceScheme2 if scheme == 2 else oz.WorkspaceScheme1)(executor, M, N, K, S, materialize=materialize)
+    want = _device_result(executor, 2, A, B, S, True)
+    W = oz.WorkspaceScheme2(executor, M, N, K, S, materialize=True)
     C = np.empty((M, N))
     oz.ozaki_gemm_host(W, A, B, C)
     assert np.array_equal(C.view(np.int64), want.view(np.int64))
