@@ -584,13 +584,15 @@ def run_precision_suite(args, local):
         dms = time_events(lambda: torch.matmul(dA, dB, out=dD), 5, stream)
         target = oz.block_error(ex, dA, dB, dD, M, N, K, block, tune_seed)
         dgemm_val = oz.block_error(ex, dA, dB, dD, M, N, K, block, val_seed)
+        dgemm_more = {sd: oz.block_error(ex, dA, dB, dD, M, N, K, block, sd) for sd in range(3, 11)}
         flops = 2.0 * M * N * K
         # the accuracy knob's own choice of scheme and count for this target
         t0 = time.perf_counter()
         try:
-            chosen = oz.autotune_scheme(ex, dA, dB, M, N, K, target, block, tune_seed)[:2]
+            knob = oz.autotune_scheme(ex, dA, dB, M, N, K, target, block, tune_seed)
+            chosen, knob_err = tuple(knob[:2]), knob[2]
         except oz.OzaError:
-            chosen = (None, None)
+            chosen, knob_err = (None, None), None
         choose_s = time.perf_counter() - t0
         for scheme in (2, 1):
             t0 = time.perf_counter()
@@ -618,6 +620,10 @@ def run_precision_suite(args, local):
             Dr = dD.index_select(0, sub).index_select(1, subc).contiguous()
             scaled = oz.block_error(ex, Ar, Bc, Cr, len(ra), len(cb), K, 64, 0)
             scaled_d = oz.block_error(ex, Ar, Bc, Dr, len(ra), len(cb), K, 64, 0)
+            # eight more independent blocks: how often the result meets DGEMM's
+            # error block by block (the largest error over a block is heavy-tailed)
+            more = [(oz.block_error(ex, dA, dB, dC, M, N, K, block, sd), dgemm_more[sd])
+                    for sd in range(3, 11)]
             line = {
                 "suite": "precision", "metric": METRIC, "value": flops / (ms * 1e-3) / 1e12, "unit": UNIT,
                 "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
@@ -628,8 +634,11 @@ def run_precision_suite(args, local):
                            "input_seed": 42},
                 "slices": S, "target_met_on_tuning_block": met,
                 "chosen_by_knob": chosen == (scheme, S), "knob_choice": {"scheme": chosen[0], "slices": chosen[1],
+                                                                         "sampled_err": knob_err,
                                                                          "autotune_scheme_s": choose_s},
                 "validation_meets_dgemm": bool(val <= dgemm_val),
+                "more_blocks_meeting_dgemm": f"{sum(o <= d for o, d in more)} of {len(more)}",
+                "more_blocks_err_ratio_max": max(o / d if d > 0 else float('inf') for o, d in more),
                 "target_rel_err": target, "tuned_block_err": tuned,
                 "validation_err": val, "cublas_dgemm_validation_err": dgemm_val,
                 "scaled_entries_err": scaled, "cublas_dgemm_scaled_entries_err": scaled_d,
