@@ -589,7 +589,8 @@ def run_precision_suite(args, local):
         # the accuracy knob's own choice of scheme and count for this target
         t0 = time.perf_counter()
         try:
-            knob = oz.autotune_scheme(ex, dA, dB, M, N, K, target, block, tune_seed)
+            # native DGEMM's error block by block: the config's target
+            knob = oz.autotune_scheme_like(ex, dA, dB, M, N, K, dD, 1.0, block, tune_seed)
             chosen, knob_err = tuple(knob[:2]), knob[2]
         except oz.OzaError:
             chosen, knob_err = (None, None), None
@@ -634,7 +635,8 @@ def run_precision_suite(args, local):
                            "input_seed": 42},
                 "slices": S, "target_met_on_tuning_block": met,
                 "chosen_by_knob": chosen == (scheme, S), "knob_choice": {"scheme": chosen[0], "slices": chosen[1],
-                                                                         "sampled_err": knob_err,
+                                                                         "call": "oza_autotune_scheme_like (C_ref = DGEMM's C)",
+                                                                         "sampled_err_ratio": knob_err,
                                                                          "autotune_scheme_s": choose_s},
                 "validation_meets_dgemm": bool(val <= dgemm_val),
                 "more_blocks_meeting_dgemm": f"{sum(o <= d for o, d in more)} of {len(more)}",

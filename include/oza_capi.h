@@ -334,6 +334,17 @@ oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, co
                                  double target_rel_err, int block, unsigned seed, int* scheme, int* slices,
                                  double* achieved_err);
 
+/* As oza_autotune_scheme, with the target given block by block by another
+ * result of the same product: C_ref (M x N device, row-major; e.g. native
+ * DGEMM's C).  A count is accepted when, on every sampled block, its maximum
+ * relative error is at most `factor` times C_ref's on that block (blocks
+ * where C_ref is exact count it as one unit roundoff).  *achieved_ratio: the
+ * largest sampled error / (factor x C_ref's), <= 1 when met.  Extension: the
+ * reference leaves scheme and slices to the caller. */
+oza_status_t oza_autotune_scheme_like(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                                      const double* C_ref, double factor, int block, unsigned seed, int* scheme,
+                                      int* slices, double* achieved_ratio);
+
 /* Slice count for a maximum-relative-error target without running anything:
  * a table measured on B200 (ozablas_b200/calibrate_slices.py) for K = 128 ..
  * 65536 and inputs (U - 0.5) * exp(phi * N(0,1)), phi = 0.5 .. 4, errors over

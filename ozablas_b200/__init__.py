@@ -158,6 +158,8 @@ def lib() -> ctypes.CDLL:
         "oza_scheme_for_target": (I, [ctypes.c_double, S, ctypes.c_double, ctypes.POINTER(I)]),
         "oza_autotune_scheme": (I, [P, S, S, S, P, P, ctypes.c_double, I, U, ctypes.POINTER(I), ctypes.POINTER(I),
                                     ctypes.POINTER(ctypes.c_double)]),
+        "oza_autotune_scheme_like": (I, [P, S, S, S, P, P, P, ctypes.c_double, I, U, ctypes.POINTER(I),
+                                         ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -600,6 +602,20 @@ def autotune_scheme(executor, A, B, M: int, N: int, K: int, target_rel_err: floa
     _check(lib().oza_autotune_scheme(executor.handle, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
                                      ctypes.c_void_p(_ptr(B)), float(target_rel_err), int(block), int(seed),
                                      ctypes.byref(sc), ctypes.byref(s), ctypes.byref(e)))
+    return sc.value, s.value, e.value
+
+
+def autotune_scheme_like(executor, A, B, M: int, N: int, K: int, C_ref, factor: float = 1.0, block: int = 96,
+                         seed: int = 7):
+    """Scheme and slice count whose error is at most factor times C_ref's
+    (another result of A @ B, e.g. native DGEMM's) on every sampled block, with
+    the fewest INT8 GEMMs; returns (scheme, slices, largest sampled error
+    ratio).  Raises OzaError if neither scheme reaches it."""
+    sc, s = ctypes.c_int(), ctypes.c_int()
+    e = ctypes.c_double()
+    _check(lib().oza_autotune_scheme_like(executor.handle, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
+                                          ctypes.c_void_p(_ptr(B)), ctypes.c_void_p(_ptr(C_ref)), float(factor),
+                                          int(block), int(seed), ctypes.byref(sc), ctypes.byref(s), ctypes.byref(e)))
     return sc.value, s.value, e.value
 
 

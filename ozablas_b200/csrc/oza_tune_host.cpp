@@ -73,6 +73,7 @@ struct Block {
     double* Cb = nullptr;
     double* Rb = nullptr;
     std::vector<double> ref;
+    double unit = 1.0;   // errors on this block are compared in units of this (a reference result's error)
     ~Block() {
         void* bufs[] = {d_idx, Ab, Bb, Cb, Rb};
         for (void* p : bufs)
@@ -137,6 +138,7 @@ oza_status_t blocks_trial(Block* const* blocks, int nblocks, int scheme, int sli
         double e = 0.0;
         const oza_status_t st = block_trial(*blocks[i], scheme, slices, &e);
         if (st != OZA_OK) return st;
+        e /= blocks[i]->unit;
         if (!(e <= worst)) worst = e;   // NaN propagates
     }
     *err = worst;
@@ -176,6 +178,19 @@ oza_status_t bisect_slices(Block* const* blocks, int nblocks, int scheme, int sm
     return OZA_OK;
 }
 
+// The error of an M x N device result C on the block's entries.
+oza_status_t given_error(const Block& b, const double* C, size_t N, double* err) {
+    std::vector<double> got((size_t)b.r * b.c);
+    std::vector<double> row(N);
+    for (int i = 0; i < b.r; ++i) {
+        const oza_status_t st = oza_executor_copy(b.ex, row.data(), C + (size_t)b.rows[i] * N, N * sizeof(double), 2);
+        if (st != OZA_OK) return st;
+        for (int j = 0; j < b.c; ++j) got[(size_t)i * b.c + j] = row[b.cols[j]];
+    }
+    *err = max_rel(got, b.ref);
+    return OZA_OK;
+}
+
 // INT8 GEMMs per Ozaki GEMM: S (Scheme II), S (S + 1) / 2 (Scheme I).
 int gemm_count(int scheme, int S) { return scheme == OZA_SCHEME2 ? S : S * (S + 1) / 2; }
 
@@ -202,6 +217,64 @@ int table_slices(const Table& tab, double target_rel_err, size_t K, double phi) 
     return S > 21 ? 21 : S;
 }
 
+// The scheme choice shared by oza_autotune_scheme and
+// oza_autotune_scheme_like.  Errors are in each block's unit and compared
+// with `target`; prepare(seed, block) samples a block.  Two independent
+// blocks: a count is accepted only if it meets the target on both, so a count
+// that just reaches it on one sample (the largest error over many outputs is
+// heavy-tailed) is not taken.  Scheme II first (S INT8 GEMMs for S moduli);
+// Scheme I (S (S + 1) / 2 GEMMs) where it is cheaper for the target or where
+// Scheme II's 20 moduli miss it.  Scheme II's moduli are also capped by its
+// INT32 bound.
+template <class Prepare>
+oza_status_t choose_scheme(const char* who, size_t K, double target, unsigned seed, Prepare prepare, int* scheme,
+                           int* slices, double* achieved) {
+    Block b0, b1;
+    oza_status_t st = prepare(seed, b0);
+    if (st == OZA_OK) st = prepare(seed ^ 0x5bd1e995u, b1);
+    if (st != OZA_OK) return st;
+    Block* blocks[2] = {&b0, &b1};
+    int S2 = 20, S1 = 20;
+    double e2 = 0.0, e1 = 0.0;
+    bool r2 = false, r1 = false;
+    const bool two_ok = (double)K * 125.0 * 125.0 < 2147483648.0;
+    if (two_ok && (st = bisect_slices(blocks, 2, OZA_SCHEME2, 20, target, &S2, &e2, &r2)) != OZA_OK) return st;
+    if (r2 && S2 == 20) {
+        // Scheme II reaches the target only at its last modulus, with no count
+        // left to add: confirm on four more blocks before taking it.
+        for (unsigned k = 1; k <= 4 && r2; ++k) {
+            Block extra;
+            if ((st = prepare(seed + 0x9e3779b9u * k, extra)) != OZA_OK) return st;
+            Block* one[1] = {&extra};
+            double e = 0.0;
+            if ((st = blocks_trial(one, 1, OZA_SCHEME2, 20, &e)) != OZA_OK) return st;
+            if (!(e <= e2)) e2 = e;
+            r2 = e2 <= target;
+        }
+    }
+    int s1max = 20;
+    if (r2)
+        while (s1max > 0 && gemm_count(OZA_SCHEME1, s1max) >= S2) --s1max;   // only a cheaper Scheme I counts
+    if (s1max > 0 && (st = bisect_slices(blocks, 2, OZA_SCHEME1, s1max, target, &S1, &e1, &r1)) != OZA_OK)
+        return st;
+    if (r1 || (!r2 && s1max > 0 && (!two_ok || e1 <= e2))) {
+        *scheme = OZA_SCHEME1;
+        *slices = S1;
+        if (achieved) *achieved = e1;
+    } else {
+        *scheme = OZA_SCHEME2;
+        *slices = S2;
+        if (achieved) *achieved = e2;
+    }
+    if (!r1 && !r2) {
+        char m[220];
+        snprintf(m, sizeof(m), "%s: target %.3g not reached with 20 slices of either scheme "
+                 "(sampled errors %.3g / %.3g)", who, target, e2, e1);
+        return tfail(OZA_UNSUPPORTED, m);
+    }
+    return OZA_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -216,15 +289,7 @@ oza_status_t oza_block_error(oza_exec_t ex, const double* A, const double* B, co
     Block b;
     oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b);
     if (st != OZA_OK) return st;
-    std::vector<double> got((size_t)b.r * b.c);
-    for (int i = 0; i < b.r; ++i) {
-        std::vector<double> row(N);
-        st = oza_executor_copy(ex, row.data(), C + (size_t)b.rows[i] * N, N * sizeof(double), 2);
-        if (st != OZA_OK) return st;
-        for (int j = 0; j < b.c; ++j) got[(size_t)i * b.c + j] = row[b.cols[j]];
-    }
-    *max_rel_err = max_rel(got, b.ref);
-    return OZA_OK;
+    return given_error(b, C, N, max_rel_err);
 }
 
 oza_status_t oza_autotune_slices(oza_exec_t ex, int scheme, size_t M, size_t N, size_t K, const double* A,
@@ -268,57 +333,32 @@ oza_status_t oza_autotune_scheme(oza_exec_t ex, size_t M, size_t N, size_t K, co
         if (achieved_err) *achieved_err = 0.0;
         return OZA_OK;
     }
-    // Two independent seeded blocks: a count is accepted only if it meets the
-    // target on both, so a count that just reaches it on one sample (the
-    // largest error over many outputs is heavy-tailed) is not taken.
-    Block b0, b1;
-    oza_status_t st = make_block(ex, A, B, M, N, K, block, seed, b0);
-    if (st == OZA_OK) st = make_block(ex, A, B, M, N, K, block, seed ^ 0x5bd1e995u, b1);
-    if (st != OZA_OK) return st;
-    Block* blocks[2] = {&b0, &b1};
-    // Scheme II first (S INT8 GEMMs for S moduli); Scheme I (S (S + 1) / 2
-    // GEMMs) where it is cheaper for the target or where Scheme II's 20
-    // moduli miss it.  Scheme II's moduli are also capped by its INT32 bound.
-    int S2 = 20, S1 = 20;
-    double e2 = 0.0, e1 = 0.0;
-    bool r2 = false, r1 = false;
-    const bool two_ok = (double)K * 125.0 * 125.0 < 2147483648.0;
-    if (two_ok && (st = bisect_slices(blocks, 2, OZA_SCHEME2, 20, target_rel_err, &S2, &e2, &r2)) != OZA_OK)
-        return st;
-    if (r2 && S2 == 20) {
-        // Scheme II reaches the target only at its last modulus, with no count
-        // left to add: confirm on four more blocks before taking it (the
-        // largest relative error over many outputs is heavy-tailed).
-        for (unsigned k = 1; k <= 4 && r2; ++k) {
-            Block extra;
-            if ((st = make_block(ex, A, B, M, N, K, block, seed + 0x9e3779b9u * k, extra)) != OZA_OK) return st;
-            double e = 0.0;
-            if ((st = block_trial(extra, OZA_SCHEME2, 20, &e)) != OZA_OK) return st;
-            if (!(e <= e2)) e2 = e;
-            r2 = e2 <= target_rel_err;
-        }
-    }
-    int s1max = 20;
-    if (r2)
-        while (s1max > 0 && gemm_count(OZA_SCHEME1, s1max) >= S2) --s1max;   // only a cheaper Scheme I counts
-    if (s1max > 0 && (st = bisect_slices(blocks, 2, OZA_SCHEME1, s1max, target_rel_err, &S1, &e1, &r1)) != OZA_OK)
-        return st;
-    if (r1 || (!r2 && s1max > 0 && (!two_ok || e1 <= e2))) {
-        *scheme = OZA_SCHEME1;
-        *slices = S1;
-        if (achieved_err) *achieved_err = e1;
-    } else {
+    auto prepare = [&](unsigned sd, Block& b) { return make_block(ex, A, B, M, N, K, block, sd, b); };
+    return choose_scheme("oza_autotune_scheme", K, target_rel_err, seed, prepare, scheme, slices, achieved_err);
+}
+
+oza_status_t oza_autotune_scheme_like(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                                      const double* C_ref, double factor, int block, unsigned seed, int* scheme,
+                                      int* slices, double* achieved_ratio) {
+    if (!ex || !A || !B || !C_ref || !scheme || !slices)
+        return tfail(OZA_INVALID_ARG, "oza_autotune_scheme_like: null argument");
+    if (!(factor > 0.0)) return tfail(OZA_INVALID_ARG, "oza_autotune_scheme_like: factor must be > 0");
+    if (M == 0 || N == 0 || K == 0) {
         *scheme = OZA_SCHEME2;
-        *slices = S2;
-        if (achieved_err) *achieved_err = e2;
+        *slices = 1;
+        if (achieved_ratio) *achieved_ratio = 0.0;
+        return OZA_OK;
     }
-    if (!r1 && !r2) {
-        char m[200];
-        snprintf(m, sizeof(m), "oza_autotune_scheme: target %.3g not reached with 20 slices of either scheme "
-                 "(sampled errors %.3g / %.3g)", target_rel_err, e2, e1);
-        return tfail(OZA_UNSUPPORTED, m);
-    }
-    return OZA_OK;
+    // Each block's errors in units of factor x the reference result's error
+    // on that block (at least one unit roundoff, for blocks it gets exact).
+    auto prepare = [&](unsigned sd, Block& b) {
+        oza_status_t st = make_block(ex, A, B, M, N, K, block, sd, b);
+        double e = 0.0;
+        if (st == OZA_OK) st = given_error(b, C_ref, N, &e);
+        if (st == OZA_OK) b.unit = factor * std::max(e, 0x1p-53);
+        return st;
+    };
+    return choose_scheme("oza_autotune_scheme_like", K, 1.0, seed, prepare, scheme, slices, achieved_ratio);
 }
 
 int oza_slices_for_target(double target_rel_err, size_t K, double phi) {

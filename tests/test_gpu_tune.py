@@ -137,3 +137,23 @@ def test_autotune_scheme_choice(executor, K, phi, target):
     elif e2(19) <= target:   # Scheme II below its cap: taken unless Scheme I is cheaper
         assert scheme == 2 or S * (S + 1) // 2 < 19
     # else Scheme II only at its cap, where the knob checks more blocks: either scheme
+
+
+@pytest.mark.parametrize("K,phi", [(2048, 0.5), (16384, 4.0)])
+def test_autotune_scheme_like_dgemm(executor, K, phi):
+    """oza_autotune_scheme_like: the chosen count's error is at most native
+    DGEMM's on each sampled block (the ratio it reports is <= 1), and at that
+    count the scheme's result does meet DGEMM's error on the knob's first
+    block."""
+    import torch
+    M, N = 128, 128
+    A = oz.generate_matrix(M, K, phi=phi, seed=61)
+    B = oz.generate_matrix(K, N, phi=phi, seed=62)
+    dA, dB = _dev(A), _dev(B)
+    D = torch.matmul(dA, dB)
+    scheme, S, ratio = oz.autotune_scheme_like(executor, dA, dB, M, N, K, D, 1.0, block=64, seed=5)
+    assert scheme in (1, 2) and 1 <= S <= 20 and ratio <= 1.0
+    C = _run(executor, scheme, A, B, S)
+    ours = oz.block_error(executor, dA, dB, _dev(C), M, N, K, block=64, seed=5)
+    dgemm = oz.block_error(executor, dA, dB, D, M, N, K, block=64, seed=5)
+    assert ours <= max(dgemm, 2.0 ** -53)
