@@ -411,9 +411,9 @@ oza_status_t oza_ws_create(oza_exec_t ex, int scheme, size_t M, size_t N, size_t
     ws->Mp = oza::round_up(M, oza::kTileM);
     ws->Np = oza::round_up(N, oza::kTileN);
     ws->Kp = oza::round_up(K, oza::kTileK);
-    ws->groups = slices;
     ws->flags = flags;
-    ws->pairs = oza::make_pairs(scheme, slices);
+    ws->pairs = oza::make_pairs(scheme, slices, K);
+    ws->groups = ws->pairs.num_groups;   // INT32 planes: Scheme I groups may split at large K
     if (scheme == OZA_SCHEME2) ws->k_param = K ? oza_scheme2_k_param(slices, K) : 0;
     else ws->beta = K ? oza_scheme1_beta(K) : 1;
 
@@ -618,17 +618,19 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
                          "step4 crt");
         } else {
             OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc, ws->Mp, ws->Np, M, N, ws->S, ws->beta, ws->shiftA,
-                                                  ws->shiftB, C, ex->sms, st),
+                                                  ws->shiftB, C, ex->sms, st, &ws->pairs),
                          "step4 sum");
         }
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[4], st), "CUDA: event record");
         if (ws->a_ref) {
             // OZA_WS_REFERENCE_LAYOUT: the reference's buffers, outside the timed steps.
-            const int c_first = ws->scheme == OZA_SCHEME2 ? 0 : ws->groups - 1;
-            const int c_count = ws->scheme == OZA_SCHEME2 ? ws->groups : 1;
+            // Scheme I: the last group (its planes summed where it was split)
+            const bool s2 = ws->scheme == OZA_SCHEME2;
+            const int c_first = s2 ? 0 : ws->pairs.first_unit[ws->S - 1];
+            const int c_count = s2 ? ws->groups : ws->groups - c_first;
             OZA_CUDA_TRY(oza::launch_to_reference_layout(ws->aplanes, ws->bplanes, ws->ctc, ws->S, ws->groups, M, N,
                                                          K, ws->Mp, ws->Np, ws->Kp, ws->a_ref, ws->b_ref, ws->c_ref,
-                                                         c_first, c_count, st),
+                                                         c_first, c_count, !s2, st),
                          "reference-layout copies");
         }
     }
@@ -795,7 +797,8 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
                              "step4 crt");
             } else {
                 OZA_CUDA_TRY(oza::launch_reconstruct1(ws->ctc + r0 * ws->Np, ws->Mp, ws->Np, rows, N, ws->S, ws->beta,
-                                                      ws->shiftA + r0, ws->shiftB, h.dC + r0 * N, ex->sms, st),
+                                                      ws->shiftA + r0, ws->shiftB, h.dC + r0 * N, ex->sms, st,
+                                                      &ws->pairs),
                              "step4 sum");
             }
             OZA_CUDA_TRY(cudaEventRecord(h.done[c], st), "CUDA: event record");

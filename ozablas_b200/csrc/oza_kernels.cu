@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <initializer_list>
 #include <memory>
@@ -184,29 +185,43 @@ cudaError_t upload_tables() {
     return cudaSuccess;
 }
 
-PairList make_pairs(int scheme, int slices) {
+PairList make_pairs(int scheme, int slices, size_t K) {
     PairList p{};
-    int n = 0;
-    p.num_groups = slices;
+    int n = 0, u = 0;
+    // Scheme I: pairs per INT32 accumulator, from |slice| <= 2^(beta - 1)
+    int per_unit = 1 << 30;
+    if (scheme != 2 && K > 0) {
+        int beta = (int)std::floor((31.0 - std::log2((double)K)) / 2.0);
+        beta = beta < 1 ? 1 : (beta > 7 ? 7 : beta);
+        const double bound = (double)K * std::ldexp(1.0, 2 * beta - 2);
+        const double fit = std::floor(2147483647.0 / bound);
+        per_unit = fit < 1.0 ? 1 : (fit > 1e9 ? 1 << 30 : (int)fit);
+    }
     for (int g = 0; g < slices; ++g) {
-        p.start[g] = n;
+        p.first_unit[g] = u;
         if (scheme == 2) {
+            p.start[u++] = n;
             p.a[n] = (uint8_t)g;
             p.b[n] = (uint8_t)g;
             ++n;
         } else {
             // group g+2 (1-based slices s + t = g + 2), reference pipeline.cu:102-126
-            int G = g + 2;
+            const int G = g + 2;
+            int in_unit = 0;
             for (int s = 1; s <= G - 1; ++s) {
-                int t = G - s;
+                const int t = G - s;
                 if (s > slices || t > slices) continue;
+                if (in_unit == 0) p.start[u++] = n;
                 p.a[n] = (uint8_t)(s - 1);
                 p.b[n] = (uint8_t)(t - 1);
                 ++n;
+                if (++in_unit == per_unit) in_unit = 0;
             }
         }
     }
-    p.start[slices] = n;
+    p.first_unit[slices] = u;
+    p.start[u] = n;
+    p.num_groups = u;
     return p;
 }
 
@@ -1299,6 +1314,71 @@ __global__ void __launch_bounds__(256) k_reconstruct1(const int32_t* __restrict_
         reconstruct1_chunk<S>(ctc, Np, N, plane, beta, negA, negB, C, w.r, w.c);
 }
 
+// Scheme I step 4 where some groups were split over several INT32 planes
+// (large K: make_pairs): group g's value is the exact sum of its planes
+// [first[g], first[g + 1]), formed in 64 bits -- equal to the reference's
+// INT32 group sum wherever that one does not overflow -- then the same
+// scaled fused multiply-add in g order as k_reconstruct1.
+struct UnitMap {
+    int first[kMaxSlicesHost + 1];
+};
+__global__ void __launch_bounds__(256) k_reconstruct1_units(const int32_t* __restrict__ ctc, long long Mp,
+                                                            long long Np, long long M, long long N, int S, int beta,
+                                                            const int32_t* __restrict__ negA,
+                                                            const int32_t* __restrict__ negB,
+                                                            double* __restrict__ C, const __grid_constant__ UnitMap um) {
+    const size_t plane4 = ((size_t)Mp * (size_t)Np) >> 2;
+    for (GridWalk w((long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, (N + 3) >> 2);
+         w.r < M; w.next()) {
+        const long long i = w.r, j0 = w.c << 2;
+        const int4* src = reinterpret_cast<const int4*>(ctc + (size_t)i * Np + j0);
+        const double ui = ldexp(1.0, -negA[i] + 1 - beta);
+        double uv[4], acc[4] = {0.0, 0.0, 0.0, 0.0};
+        int lim[4];
+        for (int e = 0; e < 4; ++e) {
+            const long long j = j0 + e;
+            uv[e] = __dmul_rn(ui, ldexp(1.0, (j < N ? -negB[j] : 0) + 1 - beta));
+            const int E = (int)((unsigned long long)__double_as_longlong(uv[e]) >> 52) & 0x7FF;
+            lim[e] = (E == 0 || E == 0x7FF) ? 0x7FFFFFFF : -1022 - (E - 1023);
+        }
+        for (int g = 0; g < S; ++g) {
+            long long sum[4] = {0, 0, 0, 0};
+            for (int u = um.first[g]; u < um.first[g + 1]; ++u) {
+                const int4 v = __ldg(src + (size_t)u * plane4);
+                sum[0] += v.x;
+                sum[1] += v.y;
+                sum[2] += v.z;
+                sum[3] += v.w;
+            }
+            const int k = -beta * g;
+            const double p = __longlong_as_double((long long)(k + 1023) << 52);
+            for (int e = 0; e < 4; ++e) {
+                const double scale = k >= lim[e] ? __dmul_rn(uv[e], p) : ldexp_outlined(uv[e], k);
+                acc[e] = __fma_rn((double)sum[e], scale, acc[e]);
+            }
+        }
+        double* crow = C + i * N;
+        for (int e = 0; e < 4; ++e)
+            if (j0 + e < N) crow[j0 + e] = acc[e];
+    }
+}
+
+// Sum of planes [first, first + count) of ctc (Mp x Np) into dst (M x N,
+// row-major), in two's-complement 32-bit arithmetic: the INT32 buffer the
+// reference's consecutive GEMMs with beta = 1 leave.
+__global__ void __launch_bounds__(256) k_sum_planes(const int32_t* __restrict__ ctc, long long Mp, long long Np,
+                                                    long long M, long long N, int first, int count,
+                                                    int32_t* __restrict__ dst) {
+    const size_t plane = (size_t)Mp * (size_t)Np;
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M * N;
+         id += (long long)gridDim.x * blockDim.x) {
+        const long long i = id / N, j = id - i * N;
+        uint32_t s = 0;
+        for (int u = first; u < first + count; ++u) s += (uint32_t)ctc[(size_t)u * plane + (size_t)i * Np + j];
+        dst[id] = (int32_t)s;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Grouped Scheme II: steps 1, 2 and 4 of many independent GEMMs, one launch
 // per stage (per slice-count class for the templated stages).  Block b of a
@@ -1683,12 +1763,20 @@ cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M,
 }
 
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
-                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st) {
+                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st,
+                                const PairList* units) {
     const long long total = (long long)M * (long long)((N + 3) / 4);
     if (total == 0) return cudaSuccess;
     if (Np % 4 != 0 || beta < 1 || beta * S > 1022) return cudaErrorInvalidValue;
     const int grid = grid_for(total, 256, sms, 16);
     const long long MP = (long long)Mp, NP = (long long)Np, MM = (long long)M, NN = (long long)N;
+    if (units && units->num_groups != S) {
+        if (S < 1 || S > kMaxSlicesHost || units->first_unit[S] != units->num_groups) return cudaErrorInvalidValue;
+        UnitMap um{};
+        for (int g = 0; g <= S; ++g) um.first[g] = units->first_unit[g];
+        k_reconstruct1_units<<<grid, 256, 0, st>>>(ctc, MP, NP, MM, NN, S, beta, negA, negB, C, um);
+        return cudaGetLastError();
+    }
     switch (S) {
 #define OZA_CASE(n) \
     case n: k_reconstruct1<n><<<grid, 256, 0, st>>>(ctc, MP, NP, MM, NN, beta, negA, negB, C); break;
@@ -1992,7 +2080,7 @@ cudaError_t group_plan_launch(GroupPlan* p, unsigned long long* colmax, size_t c
 cudaError_t launch_to_reference_layout(const int8_t* a_planes, const int8_t* b_planes, const int32_t* ctc, int S,
                                       int groups, size_t M, size_t N, size_t K, size_t Mp, size_t Np, size_t Kp,
                                       int8_t* a_ref, int8_t* b_ref, int32_t* c_ref, int c_first, int c_count,
-                                      cudaStream_t st) {
+                                      bool sum_planes, cudaStream_t st) {
     if (M == 0 || N == 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     for (int s = 0; s < S && K && e == cudaSuccess; ++s)
@@ -2005,6 +2093,11 @@ cudaError_t launch_to_reference_layout(const int8_t* a_planes, const int8_t* b_p
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (c_first < 0 || c_count < 0 || c_first + c_count > groups) return cudaErrorInvalidValue;
+    if (sum_planes && c_count > 1) {
+        k_sum_planes<<<grid_for((long long)(M * N), 256, 148, 8), 256, 0, st>>>(
+            ctc, (long long)Mp, (long long)Np, (long long)M, (long long)N, c_first, c_count, c_ref);
+        return cudaGetLastError();
+    }
     for (int g = 0; g < c_count && e == cudaSuccess; ++g)
         e = cudaMemcpy2DAsync(c_ref + (size_t)g * M * N, N * sizeof(int32_t), ctc + (size_t)(c_first + g) * Mp * Np,
                               Np * sizeof(int32_t), N * sizeof(int32_t), M, cudaMemcpyDeviceToDevice, st);

@@ -21,13 +21,20 @@ inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 // Which (A-plane, B-plane) products are summed into each INT32 group.
 // Scheme II: group s = A_s * B_s.  Scheme I: group g (plane g-2) sums
 // A_s * B_t over s + t = g (1-based slice indices), s, t <= S.
+// Accumulation units of the GEMM: Scheme II one per modulus; Scheme I one per
+// group g = s + t, split into consecutive sub-groups where the group's INT32
+// sum could overflow (more than (2^31 - 1) / (K 2^(2 beta - 2)) pairs: each
+// slice product is at most 2^(2 beta - 2) in magnitude), so every INT32
+// accumulator stays exact.  Each unit is one INT32 (or coefficient) plane.
+constexpr int kMaxUnits = 80;   // Scheme I, S = 20, at least 3 pairs per unit: 77
 struct PairList {
-    int num_groups;
-    int start[kMaxSlicesHost + 1];
+    int num_groups;                      // units
+    int start[kMaxUnits + 1];            // pairs of unit u: [start[u], start[u + 1])
+    int first_unit[kMaxSlicesHost + 1];  // Scheme I: units of group g: [first_unit[g], first_unit[g + 1])
     uint8_t a[kMaxSlicesHost * (kMaxSlicesHost + 1) / 2];
     uint8_t b[kMaxSlicesHost * (kMaxSlicesHost + 1) / 2];
 };
-PairList make_pairs(int scheme, int slices);
+PairList make_pairs(int scheme, int slices, size_t K);
 
 // Upload the per-modulus and CRT constants to the current device.
 cudaError_t upload_tables();
@@ -79,7 +86,8 @@ cudaError_t launch_reconstruct2(const int32_t* ctc, size_t Mp, size_t Np, size_t
 cudaError_t launch_crt_coef(const uint8_t* coef, size_t Mp, size_t Np, size_t M, size_t N, int S,
                             const int32_t* shiftA, const int32_t* shiftB, double* C, int sms, cudaStream_t st);
 cudaError_t launch_reconstruct1(const int32_t* ctc, size_t Mp, size_t Np, size_t M, size_t N, int S, int beta,
-                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st);
+                                const int32_t* negA, const int32_t* negB, double* C, int sms, cudaStream_t st,
+                                const PairList* units = nullptr);
 
 // Grouped Scheme II: many independent GEMMs, each stage one launch (the
 // slicers and the CRT one per slice-count class).  Buffers as in a Scheme II
@@ -121,7 +129,7 @@ int group_plan_launches(const GroupPlan* p);   // kernel launches per call
 cudaError_t launch_to_reference_layout(const int8_t* a_planes, const int8_t* b_planes, const int32_t* ctc, int S,
                                       int groups, size_t M, size_t N, size_t K, size_t Mp, size_t Np, size_t Kp,
                                       int8_t* a_ref, int8_t* b_ref, int32_t* c_ref, int c_first, int c_count,
-                                      cudaStream_t st);
+                                      bool sum_planes, cudaStream_t st);
 
 // One bounded wait on an mbarrier that nothing arrives on (self-test of the
 // wait bound): *gerr receives the device error code, *status 1 if it returned early.

@@ -123,7 +123,9 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     const size_t S = (size_t)slices;
     const size_t need_err = 256, need_sa = align256(M * 4), need_sb = align256(N * 4), need_cm = align256(N * 8);
     const size_t need_ap = align256(S * Mp * Kp + 16), need_bp = align256(S * Np * Kp + 16);
-    const size_t need_out = align256(scheme == OZA_SCHEME2 ? S * Mp * Np + 16 : S * Mp * Np * 4 + 16);
+    // Scheme I: one INT32 plane per accumulation unit (groups split at large K)
+    const size_t planes_out = scheme == OZA_SCHEME2 ? S : (size_t)oza::make_pairs(scheme, slices, K).num_groups;
+    const size_t need_out = align256(scheme == OZA_SCHEME2 ? S * Mp * Np + 16 : planes_out * Mp * Np * 4 + 16);
     const size_t need = need_err + need_sa + need_sb + need_cm + need_ap + need_bp + need_out;
     if (need > (size_t)OZA_NOALLOC_SCRATCH_BYTES) {
         char msg[256];
@@ -175,7 +177,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     plan.Mp = Mp;
     plan.Np = Np;
     plan.Kp = Kp;
-    plan.pairs = oza::make_pairs(scheme, slices);
+    plan.pairs = oza::make_pairs(scheme, slices, K);
     plan.err = err;
     plan.sms = sms;
     plan.ctc = scheme == OZA_SCHEME1 ? reinterpret_cast<int32_t*>(out) : nullptr;
@@ -185,7 +187,7 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
         NA_TRY(oza::launch_crt_coef(out, Mp, Np, M, N, slices, shiftA, shiftB, C, sms, st), "step 4");
     else
         NA_TRY(oza::launch_reconstruct1(reinterpret_cast<int32_t*>(out), Mp, Np, M, N, slices, beta, shiftA, shiftB,
-                                        C, sms, st),
+                                        C, sms, st, &plan.pairs),
                "step 4");
 #undef NA_TRY
     return OZA_OK;

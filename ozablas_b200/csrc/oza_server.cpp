@@ -123,7 +123,10 @@ struct WsLayout {
         Np = oza::round_up(N, oza::kTileN);
         Kp = oza::round_up(K, oza::kTileK);
         const size_t s = (size_t)S;
-        const size_t out = s * Mp * Np * (scheme == OZA_SCHEME1 ? sizeof(int32_t) : 1);
+        // Scheme I: one INT32 plane per accumulation unit (groups split at large K)
+        const size_t out = scheme == OZA_SCHEME1
+                               ? (size_t)oza::make_pairs(scheme, S, K).num_groups * Mp * Np * sizeof(int32_t)
+                               : s * Mp * Np;
         const size_t sz[5] = {M * 4, N * 4, s * Mp * Kp, s * Np * Kp, out};
         size_t o = 0;
         for (int i = 0; i < 5; ++i) {
@@ -348,7 +351,7 @@ bool oza_server::launch() {
         g.Mp = p.Mp;
         g.Np = p.Np;
         g.Kp = p.Kp;
-        g.pairs = oza::make_pairs(scheme, p.S);
+        g.pairs = oza::make_pairs(scheme, p.S, p.K);
         g.err = err;
         g.sms = ex->sms;
         g.ctc = scheme == OZA_SCHEME1 ? reinterpret_cast<int32_t*>(p.coef) : nullptr;
@@ -367,7 +370,7 @@ bool oza_server::launch() {
             e = oza::launch_crt_coef(p.coef, p.Mp, p.Np, p.M, p.N, p.S, p.shiftA, p.shiftB, p.C, ex->sms, sl->st);
         if (e == cudaSuccess && scheme == OZA_SCHEME1)
             e = oza::launch_reconstruct1(g.ctc, p.Mp, p.Np, p.M, p.N, p.S, beta, p.shiftA, p.shiftB, p.C, ex->sms,
-                                         sl->st);
+                                         sl->st, &g.pairs);
     } else {
         std::memcpy(sl->pinned + kAlign, oza::group_plan_image(plan), sl->tab_bytes);
         void* tab = arena_base + sl->tab_off;

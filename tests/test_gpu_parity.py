@@ -216,3 +216,29 @@ def test_all_zero_chunks_bit_exact(executor, scheme, S):
     ref = (Oracle.scheme2 if scheme == 2 else Oracle.scheme1)(A, B, S)
     _check_all(got, ref)
     _padding_zero(got)
+
+
+def test_scheme1_split_groups_vs_oracle(executor):
+    """Scheme I at K = 65536, S = 9: the groups of 8 and 9 slice pairs are
+    split over two INT32 planes each (at most 7 pairs per plane keep every
+    INT32 sum exact) and added exactly in step 4; C, shifts and slices equal
+    the oracle's, which accumulates each group in one INT32 as the reference
+    does (random data: no overflow)."""
+    oz = _oz()
+    from oracle import Oracle
+    M, N, K, S = 32, 48, 65536, 9
+    A = oz.generate_matrix(M, K, 1.0, 7)
+    B = oz.generate_matrix(K, N, 1.0, 8)
+    got = run_pipeline(oz, executor, 1, A, B, S)
+    assert got["ws"].info["groups"] == 11
+    ref = Oracle.scheme1(A, B, S)
+    assert np.array_equal(got["shift_A"], ref["shift_A"])
+    assert np.array_equal(got["shift_B"], ref["shift_B"])
+    assert np.array_equal(got["A_slices"], ref["A_slices"])
+    assert np.array_equal(got["B_slices"], ref["B_slices"])
+    # group g's planes add up to the oracle's INT32 group plane
+    first = [0, 1, 2, 3, 4, 5, 6, 7, 9, 11]
+    for g in range(S):
+        summed = got["C_tc"][first[g]:first[g + 1]].astype(np.int64).sum(axis=0)
+        assert np.array_equal(summed, ref["C_tc"][g].astype(np.int64))
+    assert np.array_equal(bits(got["C"]), bits(ref["C"]))

@@ -97,3 +97,34 @@ def test_reference_layout_getters_match_reference_buffers(executor, scheme, S):
     assert np.array_equal(grab(ws.get_C_tc(), (G, M, N), np.int32), ref["C_tc"])
     assert np.array_equal(grab(ws.get_shift_A(), (M,), np.int32), ref["shift_A"])
     assert np.array_equal(bits(dC.cpu().numpy()), bits(ref["C"]))
+
+
+def test_scheme1_split_groups_match_reference_gpu(executor):
+    """At K = 65536 (beta = 7) a Scheme I group of more than 7 slice pairs
+    could overflow an INT32 sum in the worst case, so the library splits such
+    groups over several INT32 planes and adds them exactly.  Where the
+    reference's INT32 sums do not overflow (random data), everything matches
+    it bit for bit: C, shifts, slices, and the last group's buffer, whose
+    planes are summed for the reference layout."""
+    import ctypes
+    import torch
+    oz = _oz()
+    M, N, K, S = 64, 64, 65536, 9     # groups of 8 and 9 pairs: 11 INT32 planes
+    A = oz.generate_matrix(M, K, 1.0, 42)
+    B = oz.generate_matrix(K, N, 1.0, 43)
+    ref = ref_gpu.run(executor, 1, A, B, S)
+    ws = oz.WorkspaceScheme1(executor, M, N, K, S, reference_layout=True)
+    assert ws.info["groups"] == 11
+    dC = torch.empty(M, N, dtype=torch.float64, device="cuda")
+    oz.ozaki_scheme1_gemm(ws, torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda(), dC)
+    torch.cuda.synchronize()
+
+    def grab(ptr, shape, dtype):
+        a = np.empty(shape, dtype)
+        executor.copy_to_host(a.ctypes.data_as(ctypes.c_void_p).value, ptr, a.nbytes)
+        return a
+
+    assert np.array_equal(bits(dC.cpu().numpy()), bits(ref["C"]))
+    assert np.array_equal(grab(ws.get_shift_A(), (M,), np.int32), ref["shift_A"])
+    assert np.array_equal(grab(ws.get_A_slices(), (S, M, K), np.int8), ref["A_slices"])
+    assert np.array_equal(grab(ws.get_C_tc(), (1, M, N), np.int32), ref["C_tc"])
