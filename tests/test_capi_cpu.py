@@ -235,6 +235,12 @@ def test_server_request_bytes_layout():
         assert oz.Server.request_bytes(M, N, K, S, scheme=1) == want1
     assert oz.Server.request_bytes(0, 4, 4, 8) == 0
     assert oz.Server.request_bytes(4, 4, 4, 21) == 0
+    # Scheme I at K = 65536, S = 9: the groups of 8 and 9 slice pairs take two
+    # INT32 planes each (at most 7 pairs per exact INT32 sum): 11 planes
+    M, N, K, S = 64, 64, 65536, 9
+    Mp, Np, Kp = ru(M, 128), ru(N, 256), ru(K, 128)
+    want1 = sum(ru(x, 1024) for x in (4 * M, 4 * N, S * Mp * Kp, S * Np * Kp, 4 * 11 * Mp * Np))
+    assert oz.Server.request_bytes(M, N, K, S, scheme=1) == want1
 
 
 def test_slices_for_target_is_a_monotone_lookup():
