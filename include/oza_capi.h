@@ -82,7 +82,9 @@ typedef struct oza_ws_info {
     int scheme, slices;
     size_t M, N, K;
     size_t Mp, Np, Kp;     /* padded extents used by the device layouts   */
-    int groups;            /* INT32 product planes: S (II) or S (I, one per group g=2..S+1) */
+    int groups;            /* INT32 product planes: S (II); Scheme I one per group g=2..S+1,
+                              more where a group is split into several exact INT32 sums
+                              (at most (2^31 - 1) / (K 2^(2 beta - 2)) slice pairs each) */
     int k_param;           /* Scheme II: K_param of step 1; Scheme I: 0   */
     int beta;              /* Scheme I: slice width beta; Scheme II: 0    */
     unsigned flags;

@@ -5,8 +5,10 @@
 // kernels, not as in the reference.  Slices/residues are K-major and padded
 // (zeros in the K padding; rows past M and N unwritten): get_A_slices() is
 // int8 [S][Mp][Kp], get_B_slices() is int8 [S][Np][Kp] (B transposed), get_C_tc() is int32 [S][Mp][Np] with plane g
-// holding group g (Scheme II: residue g; Scheme I: slice-sum group g+2), and
-// null for Scheme II, whose INT32 products never reach memory.  The padded
+// holding group g (Scheme II: residue g; Scheme I: slice-sum group g+2; at large K
+// a Scheme I group can span several planes, each an exact INT32 sum of some of its
+// slice pairs: oza_ws_info_t::groups planes), and null for Scheme II, whose INT32
+// products never reach memory.  The padded
 // extents are get_Mp()/get_Np()/get_Kp().  Constructed with
 // WorkspaceLayout::Reference, the getters return the reference's own layouts
 // instead, refreshed by every GEMM call: A slices [S][M][K], B slices
