@@ -363,6 +363,15 @@ int oza_slices_for_target(double target_rel_err, size_t K, double phi);
  * caller. */
 int oza_scheme_for_target(double target_rel_err, size_t K, double phi, int* slices);
 
+/* Estimate of phi, the exponent spread the two lookups above take, from the
+ * data: on `block` sampled rows of A and columns of B (device, row-major),
+ * the variance of ln|x| about each row's and column's own mean, pooled over
+ * nonzero finite entries, is 1 + phi^2 for (U - 0.5) exp(phi N(0,1)) inputs
+ * (the family the tables were calibrated on).  Row and column scaling, which
+ * the step-1 shifts absorb, does not change it.  Extension. */
+oza_status_t oza_estimate_phi(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                              int block, unsigned seed, double* phi);
+
 /* ---- host utilities ------------------------------------------------------- */
 /* Seeded test matrix (U - 0.5) * exp(phi * N(0,1)) with U in (0,1], drawn from
  * std::mt19937(seed) in row-major order.

@@ -160,6 +160,7 @@ def lib() -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_double)]),
         "oza_autotune_scheme_like": (I, [P, S, S, S, P, P, P, ctypes.c_double, I, U, ctypes.POINTER(I),
                                          ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]),
+        "oza_estimate_phi": (I, [P, S, S, S, P, P, I, U, ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -617,6 +618,15 @@ def autotune_scheme_like(executor, A, B, M: int, N: int, K: int, C_ref, factor: 
                                           ctypes.c_void_p(_ptr(B)), ctypes.c_void_p(_ptr(C_ref)), float(factor),
                                           int(block), int(seed), ctypes.byref(sc), ctypes.byref(s), ctypes.byref(e)))
     return sc.value, s.value, e.value
+
+
+def estimate_phi(executor, A, B, M: int, N: int, K: int, block: int = 96, seed: int = 7) -> float:
+    """The exponent spread phi of the calibrated tables, estimated from
+    sampled rows of A and columns of B (device matrices)."""
+    phi = ctypes.c_double()
+    _check(lib().oza_estimate_phi(executor.handle, int(M), int(N), int(K), ctypes.c_void_p(_ptr(A)),
+                                  ctypes.c_void_p(_ptr(B)), int(block), int(seed), ctypes.byref(phi)))
+    return phi.value
 
 
 def scheme_for_target(target_rel_err: float, K: int, phi: float = 2.0):

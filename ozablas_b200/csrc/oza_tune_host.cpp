@@ -361,6 +361,74 @@ oza_status_t oza_autotune_scheme_like(oza_exec_t ex, size_t M, size_t N, size_t 
     return choose_scheme("oza_autotune_scheme_like", K, 1.0, seed, prepare, scheme, slices, achieved_ratio);
 }
 
+oza_status_t oza_estimate_phi(oza_exec_t ex, size_t M, size_t N, size_t K, const double* A, const double* B,
+                              int block, unsigned seed, double* phi) {
+    if (!ex || !A || !B || !phi) return tfail(OZA_INVALID_ARG, "oza_estimate_phi: null argument");
+    if (block < 1) return tfail(OZA_INVALID_ARG, "oza_estimate_phi: block size must be >= 1");
+    *phi = 0.0;
+    if (M == 0 || N == 0 || K == 0) return OZA_OK;
+    std::mt19937_64 rng(seed);
+    const std::vector<long long> rows = sample_indices(M, block, rng), cols = sample_indices(N, block, rng);
+    const int r = (int)rows.size(), c = (int)cols.size();
+    void* d_idx = nullptr;
+    double *Ab = nullptr, *Bb = nullptr;
+    oza_status_t st = oza_executor_alloc(ex, &d_idx, (size_t)(r + c) * sizeof(long long));
+    if (st == OZA_OK) st = oza_executor_alloc(ex, (void**)&Ab, (size_t)r * K * sizeof(double) + 8);
+    if (st == OZA_OK) st = oza_executor_alloc(ex, (void**)&Bb, K * (size_t)c * sizeof(double) + 8);
+    std::vector<double> ha((size_t)r * K), hb(K * (size_t)c);
+    if (st == OZA_OK) {
+        std::vector<long long> idx(rows);
+        idx.insert(idx.end(), cols.begin(), cols.end());
+        st = oza_executor_copy(ex, d_idx, idx.data(), idx.size() * sizeof(long long), 1);
+    }
+    if (st == OZA_OK) {
+        int dev = 0, prev = -1;
+        st = oza_executor_device(ex, &dev);
+        if (st == OZA_OK) {
+            if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+            const long long* di = static_cast<const long long*>(d_idx);
+            cudaError_t e = prev != dev ? cudaSetDevice(dev) : cudaSuccess;
+            if (e == cudaSuccess) e = oza::launch_gather_block(A, B, M, N, K, di, r, di + r, c, Ab, Bb, nullptr);
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+            if (e != cudaSuccess) st = tfail(OZA_CUDA_ERROR, std::string("oza_estimate_phi: ") + cudaGetErrorString(e));
+        }
+    }
+    if (st == OZA_OK) st = oza_executor_copy(ex, ha.data(), Ab, ha.size() * sizeof(double), 2);
+    if (st == OZA_OK) st = oza_executor_copy(ex, hb.data(), Bb, hb.size() * sizeof(double), 2);
+    void* bufs[] = {d_idx, Ab, Bb};
+    for (void* q : bufs)
+        if (q) oza_executor_free(ex, q);
+    if (st != OZA_OK) return st;
+    // Pooled variance of ln|x| about each row's (A) and column's (B) own mean:
+    // per-row and per-column scaling, which the step-1 shifts absorb, drops
+    // out.  For (U - 0.5) exp(phi N(0,1)) it is 1 + phi^2 (ln|U - 0.5| has
+    // variance 1), the family the calibrated tables were measured on.
+    double ss = 0.0;
+    long long dof = 0;
+    auto strip = [&](const double* x, size_t n, size_t stride) {
+        double sum = 0.0, sq = 0.0;
+        long long cnt = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const double v = x[i * stride];
+            if (v == 0.0 || !std::isfinite(v)) continue;
+            const double l = std::log(std::fabs(v));
+            sum += l;
+            sq += l * l;
+            ++cnt;
+        }
+        if (cnt > 1) {
+            ss += sq - sum * sum / (double)cnt;
+            dof += cnt - 1;
+        }
+    };
+    for (int i = 0; i < r; ++i) strip(ha.data() + (size_t)i * K, K, 1);
+    for (int j = 0; j < c; ++j) strip(hb.data() + j, K, (size_t)c);
+    const double var = dof > 0 ? ss / (double)dof : 0.0;
+    *phi = var > 1.0 ? std::sqrt(var - 1.0) : 0.0;
+    return OZA_OK;
+}
+
 int oza_slices_for_target(double target_rel_err, size_t K, double phi) {
     if (!(target_rel_err > 0.0) || K == 0 || !(phi >= 0.0)) return 0;
     return table_slices(kSliceTable, target_rel_err, K, phi);

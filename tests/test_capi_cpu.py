@@ -138,6 +138,7 @@ def test_accuracy_tools_reject_null_arguments():
     assert L.oza_autotune_scheme_like(None, 4, 4, 4, None, None, None, 1.0, 8, 0, ctypes.byref(sc), ctypes.byref(s),
                                       ctypes.byref(e)) == oz.OZA_INVALID_ARG
     assert "oza_autotune_scheme_like: null" in L.oza_last_error_string().decode()
+    assert L.oza_estimate_phi(None, 4, 4, 4, None, None, 8, 0, ctypes.byref(e)) == oz.OZA_INVALID_ARG
 
 
 def test_group_api_rejects_bad_arguments_without_a_device():

@@ -157,3 +157,22 @@ def test_autotune_scheme_like_dgemm(executor, K, phi):
     ours = oz.block_error(executor, dA, dB, _dev(C), M, N, K, block=64, seed=5)
     dgemm = oz.block_error(executor, dA, dB, D, M, N, K, block=64, seed=5)
     assert ours <= max(dgemm, 2.0 ** -53)
+
+
+@pytest.mark.parametrize("phi", [0.5, 2.0, 4.0])
+def test_estimate_phi(executor, phi):
+    """oza_estimate_phi recovers the generator's phi from sampled rows and
+    columns, and row/column scaling (which the step-1 shifts absorb) does not
+    move it; the scheme lookup then takes the estimate."""
+    M, N, K = 256, 192, 4096
+    A = oz.generate_matrix(M, K, phi=phi, seed=71)
+    B = oz.generate_matrix(K, N, phi=phi, seed=72)
+    est = oz.estimate_phi(executor, _dev(A), _dev(B), M, N, K)
+    assert abs(est - phi) <= 0.1 * phi
+    A[3, :] *= 2.0 ** 300
+    B[:, 5] *= 2.0 ** -300
+    A[:, 7] = 0.0
+    est2 = oz.estimate_phi(executor, _dev(A), _dev(B), M, N, K)
+    assert abs(est2 - phi) <= 0.1 * phi
+    scheme, S = oz.scheme_for_target(1e-12, K, est2)
+    assert scheme in (1, 2) and 1 <= S <= 21
