@@ -229,6 +229,8 @@ oza_status_t gemm_overlapped(oza_workspace* ws, const double* A, const double* B
         plan.Mp = ws->Mp;
         plan.Np = ws->Np;
         plan.Kp = ws->Kp;
+        plan.M = ws->M;
+        plan.N = ws->N;
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
@@ -599,6 +601,8 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         plan.Mp = ws->Mp;
         plan.Np = ws->Np;
         plan.Kp = ws->Kp;
+        plan.M = ws->M;
+        plan.N = ws->N;
         plan.pairs = ws->pairs;
         plan.err = ws->err;
         plan.sms = ex->sms;
@@ -781,6 +785,8 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
             plan.Mp = ws->Mp;
             plan.Np = ws->Np;
             plan.Kp = ws->Kp;
+            plan.M = ws->M;
+            plan.N = ws->N;
             plan.pairs = ws->pairs;
             plan.err = ws->err;
             plan.sms = ex->sms;

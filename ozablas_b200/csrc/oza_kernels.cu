@@ -805,6 +805,7 @@ struct GemmArgs {
     uint32_t wait_hint;           // mbarrier suspend-time hint in ns (0: poll)
     int band;                     // m-tiles per rasterisation band
     long long Mp, Np;
+    long long M, N;               // real extents (the epilogue skips padding)
     int* err;
     int32_t* ctc;                 // kEpiI32: [groups][Mp][Np]
     uint8_t* coef;                // kEpiCoef: [S][Mp][Np] CRT coefficient bytes
@@ -874,6 +875,7 @@ struct GemmUnit {
     const CUtensorMap* tmB;
     int p0, p1, grp, mt, nt, k_blocks, S;
     long long Mp, Np;
+    long long M, N;               // real extents: padding rows and columns are never read
     int32_t* ctc;
     uint8_t* coef;
 };
@@ -896,6 +898,8 @@ struct SingleUnits {
         x.S = a->S;
         x.Mp = a->Mp;
         x.Np = a->Np;
+        x.M = a->M;
+        x.N = a->N;
         x.ctc = a->ctc;
         x.coef = a->coef;
     }
@@ -907,7 +911,7 @@ struct SingleUnits {
 // (problem, mt, nt, modulus), one tensor-map pair and one coefficient buffer
 // per problem.
 struct GroupGemmProblem {
-    long long Mp, Np;
+    long long Mp, Np, M, N;
     int k_blocks, S;
     uint8_t* coef;
 };
@@ -936,6 +940,8 @@ struct GroupUnits {
         x.S = pr.S;
         x.Mp = pr.Mp;
         x.Np = pr.Np;
+        x.M = pr.M;
+        x.N = pr.N;
         x.ctc = nullptr;
         x.coef = pr.coef;
     }
@@ -1111,7 +1117,13 @@ __device__ __forceinline__ void gemm_i8_body(const Units& src, int* err, uint32_
             }
             tc_fence_after();
             const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + acc * kAccCols;
-            epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, c0, c1);
+            // Skip this warp's quadrant when all its rows are tile padding, and
+            // the 32-column chunks past N: no later step reads those entries.
+            const long long cols_left = x.N - (long long)x.nt * kTileN;
+            int ce = c1;
+            if (cols_left < (long long)c1 * 32) ce = (int)((cols_left + 31) / 32);
+            if ((long long)x.mt * kTileM + q * 32 >= x.M) ce = c0;
+            if (ce > c0) epilogue_unit<EPI>(x.ctc, x.coef, x.Mp, x.Np, x.S, taddr, row, x.grp, x.nt, c0, ce);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -1709,6 +1721,8 @@ cudaError_t launch_gemm_i8(const GemmPlan& p, cudaStream_t st) {
     a.groups = p.pairs.num_groups;
     a.Mp = (long long)p.Mp;
     a.Np = (long long)p.Np;
+    a.M = (long long)(p.M ? p.M : p.Mp);
+    a.N = (long long)(p.N ? p.N : p.Np);
     a.err = p.err;
     a.ctc = p.ctc;
     a.coef = p.coef;
@@ -1872,7 +1886,7 @@ cudaError_t group_plan_build(const GroupProblem* in, int count, int* err, GroupP
         d.a_planes = p.a_planes;
         d.b_planes = p.b_planes;
         d.coef = p.coef;
-        gprobs[i] = GroupGemmProblem{d.Mp, d.Np, (int)(p.Kp / kTileK), p.S, p.coef};
+        gprobs[i] = GroupGemmProblem{d.Mp, d.Np, (long long)p.M, (long long)p.N, (int)(p.Kp / kTileK), p.S, p.coef};
         if (!make_plane_map(&maps[2 * i], p.a_planes, (size_t)p.S * p.Mp, p.Kp, kTileM) ||
             !make_plane_map(&maps[2 * i + 1], p.b_planes, (size_t)p.S * p.Np, p.Kp, kTileN))
             return cudaErrorInvalidValue;

@@ -65,6 +65,7 @@ struct GemmPlan {
     const int8_t* b_planes;   // [planes][Np][Kp]
     int planes;
     size_t Mp, Np, Kp;
+    size_t M = 0, N = 0;      // real extents (0: Mp, Np); the epilogue skips whole padding quadrants and chunks
     PairList pairs;
     int* err;                 // device error word
     int sms;

@@ -177,6 +177,8 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     plan.Mp = Mp;
     plan.Np = Np;
     plan.Kp = Kp;
+    plan.M = M;
+    plan.N = N;
     plan.pairs = oza::make_pairs(scheme, slices, K);
     plan.err = err;
     plan.sms = sms;

@@ -351,6 +351,8 @@ bool oza_server::launch() {
         g.Mp = p.Mp;
         g.Np = p.Np;
         g.Kp = p.Kp;
+        g.M = p.M;
+        g.N = p.N;
         g.pairs = oza::make_pairs(scheme, p.S, p.K);
         g.err = err;
         g.sms = ex->sms;
