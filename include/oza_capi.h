@@ -203,6 +203,16 @@ typedef struct {
 } oza_gemm_config_t;
 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg); /* NULL: defaults */
+/* Process-wide choice of the Scheme II step-2 residue slicer for S <= 16:
+ * OZA_SLICER_TENSOR (default) forms the digit products (sum_i d_i (256^i mod m))
+ * with tcgen05 INT8 MMAs, OZA_SLICER_CUDA_CORES with dp4a.  The residue planes
+ * are identical; the choice only changes speed.  Applies to calls issued
+ * afterwards.  Extension: the reference has one CUDA-core slicer
+ * (src/pipeline/step2_slicing.hpp:110-206). */
+#define OZA_SLICER_TENSOR 0
+#define OZA_SLICER_CUDA_CORES 1
+oza_status_t oza_set_residue_slicer(int mode);
+int oza_get_residue_slicer(void);
 oza_status_t oza_ws_get_gemm_config(oza_ws_t ws, oza_gemm_config_t* cfg);
 /* Times every configuration on this workspace with these device inputs
  * (step 3 device time, best of 2 after a warm-up), keeps the fastest on the

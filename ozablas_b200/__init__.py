@@ -27,7 +27,8 @@ __all__ = [
     "WorkspaceScheme1", "WorkspaceScheme2", "ozaki_scheme1_gemm", "ozaki_scheme2_gemm",
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
     "autotune_slices", "autotune_scheme", "GroupGemm", "Server", "slices_for_target", "scheme_for_target",
-    "ozaki_gemm_host", "selftest_wait_timeout",
+    "ozaki_gemm_host", "selftest_wait_timeout", "set_residue_slicer", "residue_slicer",
+    "OZA_SLICER_TENSOR", "OZA_SLICER_CUDA_CORES",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -161,6 +162,8 @@ def lib() -> ctypes.CDLL:
         "oza_autotune_scheme_like": (I, [P, S, S, S, P, P, P, ctypes.c_double, I, U, ctypes.POINTER(I),
                                          ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]),
         "oza_estimate_phi": (I, [P, S, S, S, P, P, I, U, ctypes.POINTER(ctypes.c_double)]),
+        "oza_set_residue_slicer": (I, [I]),
+        "oza_get_residue_slicer": (I, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -549,6 +552,20 @@ def ozaki_gemm_host(ws, A, B, C, timings: OzaTimings | None = None) -> None:
     if timings is not None:
         for f, _ in _Timings._fields_:
             setattr(timings, f, float(getattr(t, f)))
+
+
+OZA_SLICER_TENSOR, OZA_SLICER_CUDA_CORES = 0, 1
+
+
+def set_residue_slicer(mode: int) -> None:
+    """Process-wide Scheme II step-2 slicer for S <= 16: OZA_SLICER_TENSOR
+    (default; digit products on tcgen05 INT8 MMAs) or OZA_SLICER_CUDA_CORES
+    (dp4a).  Both give identical residue planes."""
+    _check(lib().oza_set_residue_slicer(int(mode)))
+
+
+def residue_slicer() -> int:
+    return int(lib().oza_get_residue_slicer())
 
 
 def selftest_wait_timeout(executor, limit_s: float = 0.2):

@@ -204,7 +204,7 @@ oza_status_t gemm_overlapped(oza_workspace* ws, const double* A, const double* B
     OZA_CUDA_TRY(cudaStreamWaitEvent(o.s_crt, o.start, 0), "CUDA: stream wait");
     OZA_CUDA_TRY(oza::launch_stats_cols(B, K, N, ws->colmax, ex->sms, st), "step1 cols");
     OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
-                                        ws->bplanes, ws->Np, ws->Kp, st),
+                                        ws->bplanes, ws->Np, ws->Kp, st, ws->err),
                  "step2 cols");
     for (int c = 0; c < R; ++c) {
         const size_t r0 = (size_t)c * q * tile_m;
@@ -213,7 +213,8 @@ oza_status_t gemm_overlapped(oza_workspace* ws, const double* A, const double* B
         OZA_CUDA_TRY(oza::launch_stats_rows(A + r0 * K, rows, K, offset, ws->shiftA + r0, ex->sms, o.s_slice),
                      "step1 rows");
         OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A + r0 * K, rows, K, ws->shiftA + r0, ws->S, ws->beta, offset,
-                                            ws->aplanes + r0 * ws->Kp, rows_p, ws->Kp, ex->sms, o.s_slice, ws->Mp),
+                                            ws->aplanes + r0 * ws->Kp, rows_p, ws->Kp, ex->sms, o.s_slice, ws->Mp,
+                                            ws->err),
                      "step2 rows");
         OZA_CUDA_TRY(cudaEventRecord(o.a_done[c], o.s_slice), "CUDA: event record");
     }
@@ -583,10 +584,10 @@ oza_status_t oza_gemm(oza_ws_t ws, const double* A, const double* B, double* C, 
         if (timings) OZA_CUDA_TRY(cudaEventRecord(ws->ev[1], st), "CUDA: event record");
         // step 2
         OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, A, M, K, ws->shiftA, ws->S, ws->beta, offset, ws->aplanes, ws->Mp,
-                                            ws->Kp, ex->sms, st),
+                                            ws->Kp, ex->sms, st, 0, ws->err),
                      "step2 rows");
         OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, B, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
-                                            ws->bplanes, ws->Np, ws->Kp, sb),
+                                            ws->bplanes, ws->Np, ws->Kp, sb, ws->err),
                      "step2 cols");
         if (dual) {
             OZA_CUDA_TRY(cudaEventRecord(ws->ov.end, sb), "CUDA: event record");
@@ -667,6 +668,15 @@ oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg) {
     ws->cfg = *cfg;
     return OZA_OK;
 }
+
+oza_status_t oza_set_residue_slicer(int mode) {
+    if (mode != OZA_SLICER_TENSOR && mode != OZA_SLICER_CUDA_CORES)
+        return fail(OZA_INVALID_ARG, "oza_set_residue_slicer: mode must be OZA_SLICER_TENSOR or OZA_SLICER_CUDA_CORES");
+    oza::set_residue_slicer(mode);
+    return OZA_OK;
+}
+
+int oza_get_residue_slicer(void) { return oza::residue_slicer(); }
 
 oza_status_t oza_ws_get_gemm_config(oza_ws_t ws, oza_gemm_config_t* cfg) {
     if (!ws || !cfg) return fail(OZA_INVALID_ARG, "oza_ws_get_gemm_config: null argument");
@@ -761,7 +771,7 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
         OZA_CUDA_TRY(cudaStreamWaitEvent(st, h.b_in, 0), "CUDA: stream wait");
         OZA_CUDA_TRY(oza::launch_stats_cols(h.dB, K, N, ws->colmax, ex->sms, st), "step1 cols");
         OZA_CUDA_TRY(oza::launch_slice_cols(ws->scheme, h.dB, K, N, ws->colmax, offset, ws->S, ws->beta, ws->shiftB,
-                                            ws->bplanes, ws->Np, ws->Kp, st),
+                                            ws->bplanes, ws->Np, ws->Kp, st, ws->err),
                      "step2 cols");
         for (int c = 0; c < R; ++c) {
             const size_t r0 = (size_t)c * q * tile_m;
@@ -776,7 +786,7 @@ oza_status_t oza_gemm_host(oza_ws_t ws, const double* hA, const double* hB, doub
                          "step1 rows");
             OZA_CUDA_TRY(oza::launch_slice_rows(ws->scheme, h.dA + r0 * K, rows, K, ws->shiftA + r0, ws->S, ws->beta,
                                                 offset, ws->aplanes + r0 * ws->Kp, rows_p, ws->Kp, ex->sms, st,
-                                                ws->Mp),
+                                                ws->Mp, ws->err),
                          "step2 rows");
             oza::GemmPlan plan;
             plan.a_planes = ws->aplanes;

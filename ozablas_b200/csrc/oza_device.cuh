@@ -24,7 +24,8 @@ enum DeviceError : int {
 //   inv    = (M/m)^-1 mod m for the current slice count (per table row)
 //   dig[w] = bytes 4w..4w+3 of (256^i mod m, symmetric, int8), i = 0..15
 //   magic32 = ceil(2^32 / m): u mod m == umulhi(u * magic32 mod 2^32, m) for u < 2^32 / m
-//   bh = m * 2^10 + (m-1)/2, adj = 256 - (m-1)/2 (residue reduction of the MMA slicer)
+//   bh = m * 2^10 + (m-1)/2, adj = 256 - (m-1)/2 (direct-remainder residue reduction)
+//   bhm = bh * magic32 mod 2^32 (the bias folded into the reduction's multiply)
 struct ModConst {
     uint32_t m;
     uint32_t magic;
@@ -32,6 +33,7 @@ struct ModConst {
     uint32_t magic32;
     int32_t bh, adj;
     uint32_t dig[4];
+    uint32_t bhm;
 };
 
 // Scheme II CRT table for one slice count S.  T = sum_s c_s (M / m_s), with
@@ -206,6 +208,11 @@ __device__ __forceinline__ void tc_fence_before() {
 }
 __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Make this thread's generic-proxy shared-memory writes visible to the async
+// proxy (the tensor core reading an operand tile written with st.shared).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // UMMA shared-memory descriptor for a K-major tile written by TMA with the

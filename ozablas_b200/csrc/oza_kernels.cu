@@ -109,6 +109,7 @@ cudaError_t upload_tables() {
         mc[s].magic32 = (uint32_t)(((1ull << 32) + m - 1) / m);
         mc[s].bh = (int32_t)(m * 1024 + (m - 1) / 2);
         mc[s].adj = (int32_t)(256 - (m - 1) / 2);
+        mc[s].bhm = (uint32_t)mc[s].bh * mc[s].magic32;
         for (int w = 0; w < 4; ++w) {
             uint32_t word = 0;
             for (int b = 0; b < 4; ++b) {
@@ -433,17 +434,53 @@ __device__ __forceinline__ int cvt_s8(double v) {
 // Kaser and Kurz, "Faster remainder by direct computation", 2019).
 // WIDE (|x| < 2^84): radix-2^21 digits and the magic division of
 // symmetric_residue.
+// Signed byte digits of x = rint(v 2^sh), |x| <= 2^62: x = sum_{i<8} d_i 256^i
+// with d_i = byte_i(x + 0x8080...80) - 128, returned as the bytes of
+// (x + 0x8080...80) ^ 0x8080...80 read as int8 (low word: d_0..d_3).
+__device__ __forceinline__ void byte_digits(double v, int sh, double p, uint32_t& lo, uint32_t& hi) {
+    const double x = rint(scale_pow2(v, sh, p));
+    const unsigned long long t = (unsigned long long)__double2ll_rn(x);
+    const unsigned long long w = (t + 0x8080808080808080ull) ^ 0x8080808080808080ull;
+    lo = (uint32_t)w;
+    hi = (uint32_t)(w >> 32);
+}
+
+// The same digits with no int64 conversion (whose conversion-unit cost bounds
+// the tensor-core slicers): for finite v and a normal p = 2^sh with |y| =
+// |v p| <= 2^62, y = yh + yl with yh = RN(y + 1.5 2^84) - 1.5 2^84 a multiple
+// of 2^32 and yl = y - yh exact in [-2^31, 2^31]; each addition of a
+// 1.5 2^k constant rounds an exact sum once, to the integer grid 2^(k-52)
+// (round half to even; yh is even in units of 2^32, so rint(y) = yh +
+// rint(yl)).  rint(yl) and yh / 2^32 are then the low words of yl + 1.5 2^52
+// and yh 2^-32 + 1.5 2^52, the high word of the former giving yl's sign.
+// FP64 pipe and integer ALU only; bit-identical to byte_digits there.
+__device__ __forceinline__ void byte_digits_fp64(double v, double p, uint32_t& lo, uint32_t& hi) {
+    const double y = __dmul_rn(v, p);
+    const double yh = __dsub_rn(__dadd_rn(y, 0x1.8p84), 0x1.8p84);
+    const double t = __dadd_rn(__dsub_rn(y, yh), 0x1.8p52);
+    const double kc = __fma_rn(yh, 0x1p-32, 0x1.8p52);
+    const uint32_t xl = (uint32_t)__double2loint(t);
+    const uint32_t xh = (uint32_t)__double2loint(kc) + ((uint32_t)__double2hiint(t) - 0x43380000u);
+    const unsigned long long x = ((unsigned long long)xh << 32) | xl;
+    const unsigned long long w = (x + 0x8080808080808080ull) ^ 0x8080808080808080ull;
+    lo = (uint32_t)w;
+    hi = (uint32_t)(w >> 32);
+}
+
+// Rows / columns whose digits byte_digits_fp64 may form: all entries finite
+// (maximum frexp exponent e <= 1024) and 2^sh a normal double.
+__device__ __forceinline__ bool fp64_digits_ok(int e, int sh) { return e <= 1024 && sh >= -1022 && sh <= 1023; }
+
 template <int S, bool WIDE, int E>
 __device__ __forceinline__ void residuesE(const double (&v)[E], int sh, double p, int8_t* dst, size_t plane_stride) {
     if constexpr (!WIDE) {
         int dlo[E], dhi[E];
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-            const double x = rint(scale_pow2(v[i], sh, p));
-            const unsigned long long t = (unsigned long long)__double2ll_rn(x);
-            const unsigned long long w = (t + 0x8080808080808080ull) ^ 0x8080808080808080ull;
-            dlo[i] = (int)(uint32_t)w;
-            dhi[i] = (int)(uint32_t)(w >> 32);
+            uint32_t lo, hi;
+            byte_digits(v[i], sh, p, lo, hi);
+            dlo[i] = (int)lo;
+            dhi[i] = (int)hi;
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -619,6 +656,317 @@ __global__ void __launch_bounds__(256, (SCHEME == 2 ? 3 : 1)) k_slice_cols(const
                                                     int S, int beta, int32_t* __restrict__ shift,
                                                     int8_t* __restrict__ out, long long Np, long long Kp) {
     slice_cols_tile<SCHEME, SC, WIDE>(B, K, N, colmax, offset, S, beta, shift, out, Np, Kp, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------------------
+// Step 2, Scheme II with S <= 16: digit products on the tensor cores
+// ---------------------------------------------------------------------------
+// The residue of x = sum_{i<8} d_i 256^i modulo m_s is the direct-remainder
+// reduction of u_s = bh_s + sum_i d_i w_{s,i}, w_{s,i} = 256^i mod m_s (int8,
+// symmetric), as in residuesE.  The sums over the digits form a small INT8
+// matrix product.  Row t of the digit tile holds the 64 digit bytes of 8
+// consecutive elements (element e at bytes 8e..8e+7); row 8s + e of the
+// weight tile holds w_{s,0..7} at bytes 8e..8e+7 and zeros elsewhere, so
+//   D[t][8s + e] = sum_i d_{t,e,i} w_{s,i}      (M = 128, N = 16 ceil(S/2), K = 64)
+// comes out of two tcgen05.mma kind::i8 (K = 32 each) into TMEM.  Thread t
+// reduces row t (one multiply-add and one mad.hi per residue) and stores 8
+// residue bytes per plane.  The two dp4a per residue of the CUDA-core slicer
+// move to the tensor pipe; the planes are bit-identical to it.
+//
+// One thread per tile row: 128 threads, warp w reads TMEM lanes 32w..32w+31;
+// 128 TMEM columns per CTA.  Shared memory, 1024-byte aligned: the digit and
+// weight tiles (128 rows x 128 B each, 128-byte swizzle, 64 B of each row
+// used), then, for the column slicer, a 32-column x 128-k FP64 tile.  A CTA's
+// dynamic shared memory (48 KB rows, 66 KB columns) keeps at most 4 (3) CTAs
+// on an SM, so their TMEM stays within 512 columns and no allocation waits,
+// and a slicer CTA never shares an SM with a GEMM CTA (198 KB).
+constexpr int kMsThreads = 128;
+constexpr int kMsTile = 128 * 128;   // one SW128 tile of 128 rows
+constexpr uint32_t kMsTmemCols = 128;
+constexpr int kMsF64Tile = 32 * 1024;
+constexpr int kMsRowsSmem = 48 * 1024;
+constexpr int kMsColsSmem = 2 * kMsTile + kMsF64Tile + 1024 /*align*/ + 64 /*barrier, slot, flag*/;
+constexpr int kMsRowsPerSm = 4;   // CTAs resident per SM: launch bounds and shared memory
+constexpr int kMsColsPerSm = 3;
+static_assert(2 * kMsTile + 1024 + 64 <= kMsRowsSmem, "row slicer shared memory");
+static_assert(5 * (kMsRowsSmem + 1024) > 228 * 1024 && 4 * (kMsColsSmem + 1024) > 228 * 1024,
+              "at most 4 (rows) / 3 (columns) slicer CTAs per SM: TMEM 512 columns");
+
+struct MsSmem {
+    uint8_t* dig;           // digit tile
+    uint8_t* wts;           // weight tile
+    uint8_t* f64;           // FP64 tile (column slicer)
+    uint64_t* bar;          // MMA completion
+    uint32_t* tmem_slot;
+    volatile int* abort;
+};
+
+__device__ __forceinline__ MsSmem ms_carve(uint8_t* raw, bool with_f64) {
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
+    MsSmem m;
+    m.dig = base;
+    m.wts = base + kMsTile;
+    m.f64 = base + 2 * kMsTile;
+    uint8_t* tail = m.f64 + (with_f64 ? kMsF64Tile : 0);
+    m.bar = reinterpret_cast<uint64_t*>(tail);
+    m.tmem_slot = reinterpret_cast<uint32_t*>(tail + 8);
+    m.abort = reinterpret_cast<volatile int*>(tail + 12);
+    return m;
+}
+
+// Row `row` of a 128-byte-swizzled tile: 16-byte chunk c at chunk c ^ (row % 8).
+__device__ __forceinline__ uint8_t* sw128_row(uint8_t* tile, int row) {
+    return tile + (row >> 3) * 1024 + (row & 7) * 128;
+}
+
+// Barrier, TMEM columns and the weight tile; returns the TMEM base address.
+template <int S>
+__device__ __forceinline__ uint32_t ms_setup(const MsSmem& m) {
+    const int t = threadIdx.x;
+    if (t == 0) {
+        mbar_init(m.bar, 1);
+        *m.abort = 0;
+        fence_barrier_init();
+    }
+    if (t < 32) {
+        tmem_alloc(m.tmem_slot, kMsTmemCols);
+        tmem_relinquish();
+    }
+    const int s = t >> 3, e = t & 7;
+    uint32_t lo = 0, hi = 0;
+    if (s < S) {
+        lo = c_mod[s].dig[0];
+        hi = c_mod[s].dig[1];
+    }
+    uint8_t* row = sw128_row(m.wts, t);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (c == (e >> 1)) {
+            if (e & 1) v.z = lo, v.w = hi;
+            else v.x = lo, v.y = hi;
+        }
+        *reinterpret_cast<uint4*>(row + ((c ^ (t & 7)) << 4)) = v;
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *m.tmem_slot;
+}
+
+__device__ __forceinline__ void ms_put_digits(uint8_t* dig, int t, const uint32_t (&lo)[8], const uint32_t (&hi)[8]) {
+    uint8_t* row = sw128_row(dig, t);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4*>(row + ((c ^ (t & 7)) << 4)) =
+            make_uint4(lo[2 * c], hi[2 * c], lo[2 * c + 1], hi[2 * c + 1]);
+}
+
+// Thread 0 issues D = digits x weights^T (two K = 32 steps) and commits to
+// the barrier; every warp then waits for it (bounded).  False if the wait gave up.
+template <int S>
+__device__ __forceinline__ bool ms_mma(const MsSmem& m, uint32_t tmem, uint32_t phase, int* err) {
+    constexpr uint32_t idesc = umma_idesc_i8(128, 16 * ((S + 1) / 2));
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        const uint64_t ad = umma_desc_sw128(smem_u32(m.dig));
+        const uint64_t bd = umma_desc_sw128(smem_u32(m.wts));
+        umma_i8(tmem, ad, bd, idesc, 0);
+        umma_i8(tmem, ad + 2, bd + 2, idesc, 1);   // +32 bytes of K
+        umma_commit(m.bar);
+    }
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) ok = mbar_wait(m.bar, phase, m.abort, err);
+    ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+    tc_fence_after();
+    return ok != 0;
+}
+
+// Residues of this thread's 8 elements from TMEM (column 8s + e holds
+// u_s(e) - bh_s); stored (when `live`) as 8 bytes per plane at dst + s plane.
+// Warp-collective: every lane calls it.
+template <int S>
+__device__ __forceinline__ void ms_store(uint32_t taddr, int8_t* dst, size_t plane, bool live) {
+#pragma unroll
+    for (int ch = 0; ch < (S + 3) / 4; ++ch) {
+        uint32_t v[32];
+        tmem_ld32(taddr + 32 * ch, v);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int s = 4 * ch + j;
+            if (s < S) {
+                const ModConst& mc = c_mod[s];
+                uint32_t r[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) r[e] = mulhi_add(v[8 * j + e] * mc.magic32 + mc.bhm, mc.m, (uint32_t)mc.adj);
+                const uint32_t w0 =
+                    __byte_perm(__byte_perm(r[0], r[1], 0x3340), __byte_perm(r[2], r[3], 0x3340), 0x5410);
+                const uint32_t w1 =
+                    __byte_perm(__byte_perm(r[4], r[5], 0x3340), __byte_perm(r[6], r[7], 0x3340), 0x5410);
+                if (live) *reinterpret_cast<uint2*>(dst + (size_t)s * plane) = make_uint2(w0, w1);
+            }
+        }
+    }
+}
+
+// After the last round: if a wait gave up, let the pending MMA finish
+// (bounded) before the TMEM columns are released.
+__device__ __forceinline__ void ms_teardown(const MsSmem& m, uint32_t tmem, uint32_t pending_phase) {
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *m.abort) {
+        volatile int no_abort = 0;
+        mbar_wait(m.bar, pending_phase, &no_abort, nullptr);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kMsTmemCols);
+    }
+}
+
+// A (rows x cols, row-major) -> out[s][plane_rows][cols_p]: a grid-stride walk
+// over (row, octet of columns), 128 octets per round.  Rows past `rows` are
+// not written, the K padding of real rows is written as zeros (as k_slice_rows).
+template <int S>
+__global__ void __launch_bounds__(kMsThreads, kMsRowsPerSm)
+    k_slice_rows_mma(const double* __restrict__ A, long long rows, long long cols, const int32_t* __restrict__ shift,
+                     int offset, int8_t* __restrict__ out, long long cols_p, long long plane_rows, int* err) {
+    extern __shared__ uint8_t ms_raw[];
+    const MsSmem m = ms_carve(ms_raw, false);
+    const uint32_t tmem = ms_setup<S>(m);
+    const int t = threadIdx.x;
+    const uint32_t taddr = tmem + ((uint32_t)(t & ~31) << 16);
+    const size_t plane = (size_t)plane_rows * (size_t)cols_p;
+    const long long octs = cols_p >> 3, total = rows * octs, stride = (long long)gridDim.x * kMsThreads;
+    GridWalk w((long long)blockIdx.x * kMsThreads + t, stride, octs);
+    // The octet of the next round is loaded while this round's MMA and
+    // reduction run (one round ahead).
+    double v[8];
+    int sh = 0;
+    auto fetch = [&](const GridWalk& at) {
+        if (at.r < rows) {
+            sh = shift[at.r];
+            const long long c0 = at.c * 8;
+            const double* src = A + at.r * cols + c0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = (c0 + i < cols) ? __ldg(src + i) : 0.0;
+        } else {
+            sh = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = 0.0;
+        }
+    };
+    fetch(w);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (long long base = (long long)blockIdx.x * kMsThreads; base < total; base += stride) {
+        const bool live = w.r < rows;
+        int8_t* dst = out + w.r * cols_p + w.c * 8;
+        uint32_t lo[8], hi[8];
+        const double p = pow2_or_zero(sh);
+        if (fp64_digits_ok(offset - sh, sh)) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) byte_digits_fp64(v[i], p, lo[i], hi[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) byte_digits(v[i], sh, p, lo[i], hi[i]);
+        }
+        ms_put_digits(m.dig, t, lo, hi);
+        w.next();
+        fetch(w);
+        fence_proxy_async_smem();
+        tc_fence_before();
+        if (!__syncthreads_and(ok)) break;
+        ok = ms_mma<S>(m, tmem, phase, err);
+        if (ok) ms_store<S>(taddr, dst, plane, live);
+        phase ^= 1;
+    }
+    ms_teardown(m, tmem, phase ^ 1);
+}
+
+// B (K x N, row-major) -> out[s][Np][Kp] (B^T, K-major), and shift[n] =
+// offset - max exponent of column n, as k_slice_cols.  Persistent over tiles
+// of 128 k x 32 n: the tile is staged through shared memory (coalesced rows
+// of B in, columns out), then 4 rounds in which thread t takes column
+// 8q + t/16 of the tile and its k-octet t % 16, so a plane's stores are 128
+// contiguous bytes per half-warp.  FP64 tile layout: column j is a 1 KB row of
+// 64 16-byte chunks (k pairs), logical chunk L stored at L ^ ((L/8 ^ j) % 8),
+// which keeps both the column-wise stores and the k-wise reads within 2x of
+// conflict-free.
+template <int S>
+__global__ void __launch_bounds__(kMsThreads, kMsColsPerSm)
+    k_slice_cols_mma(const double* __restrict__ B, long long K, long long N,
+                     const unsigned long long* __restrict__ colmax, int offset, int32_t* __restrict__ shift,
+                     int8_t* __restrict__ out, long long Np, long long Kp, int* err) {
+    extern __shared__ uint8_t ms_raw[];
+    const MsSmem m = ms_carve(ms_raw, true);
+    const uint32_t tmem = ms_setup<S>(m);
+    const int t = threadIdx.x;
+    const uint32_t taddr = tmem + ((uint32_t)(t & ~31) << 16);
+    const size_t plane = (size_t)Np * (size_t)Kp;
+    const long long tn = (N + 31) / 32, tiles = tn * (Kp / 128);
+    const int jl = t & 31, kl = t >> 5;   // staging: column jl, tile rows kl + 4i
+    const int o = t & 15;                 // rounds: k-octet
+    uint32_t phase = 0;
+    bool ok = true;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long by = tile / tn, bx = tile - by * tn;
+        const long long n0 = bx * 32, k0 = by * 128;
+        if (!__syncthreads_and(ok)) break;   // also: the previous tile's reads of the FP64 tile are done
+        {
+            const long long n = n0 + jl;
+            uint8_t* rowp = m.f64 + jl * 1024;
+#pragma unroll 8
+            for (int i = 0; i < 32; ++i) {
+                const int kk = kl + 4 * i;
+                const long long k = k0 + kk;
+                const double x = (k < K && n < N) ? __ldg(B + k * N + n) : 0.0;
+                const int L = kk >> 1;
+                *reinterpret_cast<double*>(rowp + ((L ^ (((L >> 3) ^ jl) & 7)) << 4) + ((kk & 1) << 3)) = x;
+            }
+        }
+        __syncthreads();
+        for (int q = 0; q < 4; ++q) {
+            const int j = 8 * q + (t >> 4);
+            const long long n = n0 + j;
+            const bool live = n < N;
+            int sh = 0, e = 0;
+            if (live) {
+                e = max_exp_from_bits(colmax[n]);
+                sh = offset - e;
+                if (by == 0 && o == 0) shift[n] = sh;
+            }
+            const double p = pow2_or_zero(sh);
+            const uint8_t* rowp = m.f64 + j * 1024;
+            double x[8];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int L = 4 * o + c;
+                const double2 d = *reinterpret_cast<const double2*>(rowp + ((L ^ (((L >> 3) ^ j) & 7)) << 4));
+                x[2 * c] = d.x;
+                x[2 * c + 1] = d.y;
+            }
+            uint32_t lo[8], hi[8];
+            if (fp64_digits_ok(e, sh)) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) byte_digits_fp64(x[i], p, lo[i], hi[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) byte_digits(x[i], sh, p, lo[i], hi[i]);
+            }
+            ms_put_digits(m.dig, t, lo, hi);
+            fence_proxy_async_smem();
+            tc_fence_before();
+            if (!__syncthreads_and(ok)) break;
+            ok = ms_mma<S>(m, tmem, phase, err);
+            if (ok) ms_store<S>(taddr, out + n * Kp + k0 + 8 * o, plane, live);
+            phase ^= 1;
+        }
+    }
+    ms_teardown(m, tmem, phase ^ 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -1623,14 +1971,61 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 #define OZA_FOR_EACH_S(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) \
     X(16) X(17) X(18) X(19) X(20)
 
+namespace {
+int g_residue_slicer = 0;   // 0: tensor-core digit products (S <= 16), 1: CUDA cores only
+
+template <int S>
+cudaError_t launch_rows_mma(const double* A, long long R, long long C, const int32_t* shift, int offset, int8_t* out,
+                            long long CP, long long PR, int sms, int* err, cudaStream_t st) {
+    const long long rounds = (R * (CP / 8) + kMsThreads - 1) / kMsThreads;
+    const long long cap = (long long)sms * kMsRowsPerSm;
+    const int grid = (int)(rounds < cap ? rounds : cap);
+    k_slice_rows_mma<S><<<grid, kMsThreads, kMsRowsSmem, st>>>(A, R, C, shift, offset, out, CP, PR, err);
+    return cudaGetLastError();
+}
+
+template <int S>
+cudaError_t launch_cols_mma(const double* B, long long K, long long N, const unsigned long long* colmax, int offset,
+                            int32_t* shift, int8_t* out, long long Np, long long Kp, int* err, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_slice_cols_mma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMsColsSmem);
+    });
+    if (attr != cudaSuccess) return attr;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (N + 31) / 32 * (Kp / 128);
+    const long long cap = (long long)sms * kMsColsPerSm;
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    k_slice_cols_mma<S><<<grid, kMsThreads, kMsColsSmem, st>>>(B, K, N, colmax, offset, shift, out, Np, Kp, err);
+    return cudaGetLastError();
+}
+
+#define OZA_FOR_EACH_S16(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+}  // namespace
+
+void set_residue_slicer(int mode) { g_residue_slicer = mode; }
+int residue_slicer() { return g_residue_slicer; }
+
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift, int S,
                               int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
-                              cudaStream_t st, size_t plane_rows) {
+                              cudaStream_t st, size_t plane_rows, int* err) {
     long long chunks = (long long)rows * (long long)(cols_p / (scheme == 2 ? 8 : 16));
     if (chunks == 0) return cudaSuccess;
     const int grid = grid_for(chunks, 256, sms);
     const long long R = (long long)rows, C = (long long)cols, RP = (long long)rows_p, CP = (long long)cols_p;
     const long long PR = plane_rows ? (long long)plane_rows : RP;
+    if (scheme == 2 && S <= 16 && k_param <= 62 && err && g_residue_slicer == 0) {
+        switch (S) {
+#define OZA_CASE(n) \
+    case n: return launch_rows_mma<n>(A, R, C, shift, k_param, out, CP, PR, sms, err, st);
+            OZA_FOR_EACH_S16(OZA_CASE)
+#undef OZA_CASE
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (scheme == 1) {
         k_slice_rows<1, 0, false><<<grid, 256, 0, st>>>(A, R, C, shift, S, beta, out, RP, CP, PR);
         return cudaGetLastError();
@@ -1652,11 +2047,20 @@ cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t c
 
 cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
                               int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
-                              cudaStream_t st) {
+                              cudaStream_t st, int* err) {
     if (N == 0 || Kp == 0) return cudaSuccess;
     if (N > Np) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)((N + 31) / 32), (unsigned)(Kp / 128));
     const long long KK = (long long)K, NN = (long long)N, NP = (long long)Np, KP = (long long)Kp;
+    if (scheme == 2 && S <= 16 && offset <= 62 && err && g_residue_slicer == 0) {
+        switch (S) {
+#define OZA_CASE(n) \
+    case n: return launch_cols_mma<n>(B, KK, NN, colmax, offset, shift, out, NP, KP, err, st);
+            OZA_FOR_EACH_S16(OZA_CASE)
+#undef OZA_CASE
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (scheme == 1) {
         k_slice_cols<1, 0, false><<<grid, 256, 0, st>>>(B, KK, NN, colmax, offset, S, beta, shift, out, NP, KP);
         return cudaGetLastError();

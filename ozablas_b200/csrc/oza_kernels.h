@@ -50,14 +50,21 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
 // Rows: A (rows x cols, row-major) -> out[s][rows_p][cols_p].
 // plane_rows: rows between planes of `out` (0: rows_p), so a row chunk can be
 // sliced into its place in full-size planes.
+// err: device error word; with it, Scheme II with S <= 16 forms the digit
+// products on the tensor cores (a bounded wait that expires records
+// kErrWaitTimeout there), without it on the CUDA cores.
 cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t cols, const int32_t* shift,
                               int S, int beta, int k_param, int8_t* out, size_t rows_p, size_t cols_p, int sms,
-                              cudaStream_t st, size_t plane_rows = 0);
+                              cudaStream_t st, size_t plane_rows = 0, int* err = nullptr);
 // Columns: B (K x N, row-major) -> out[s][Np][Kp] (transposed, K-major); also
 // writes shift[n] = offset - max exponent of column n.
 cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, const unsigned long long* colmax,
                               int offset, int S, int beta, int32_t* shift, int8_t* out, size_t Np, size_t Kp,
-                              cudaStream_t st);
+                              cudaStream_t st, int* err = nullptr);
+// Process-wide choice of the Scheme II residue slicer: 0 (default) tensor-core
+// digit products where S <= 16, 1 CUDA cores only.  Both give identical planes.
+void set_residue_slicer(int mode);
+int residue_slicer();
 
 // Step 3.
 struct GemmPlan {

@@ -166,9 +166,9 @@ extern "C" oza_status_t oza_gemm_noalloc(int scheme, int slices, size_t M, size_
     // oza_noalloc_device_error reads it).
     NA_TRY(oza::launch_stats_rows(A, M, K, k_param, shiftA, sms, st), "step 1 (rows)");
     NA_TRY(oza::launch_stats_cols(B, K, N, colmax, sms, st), "step 1 (columns)");
-    NA_TRY(oza::launch_slice_rows(scheme, A, M, K, shiftA, slices, beta, k_param, aplanes, Mp, Kp, sms, st),
+    NA_TRY(oza::launch_slice_rows(scheme, A, M, K, shiftA, slices, beta, k_param, aplanes, Mp, Kp, sms, st, 0, err),
            "step 2 (A)");
-    NA_TRY(oza::launch_slice_cols(scheme, B, K, N, colmax, k_param, slices, beta, shiftB, bplanes, Np, Kp, st),
+    NA_TRY(oza::launch_slice_cols(scheme, B, K, N, colmax, k_param, slices, beta, shiftB, bplanes, Np, Kp, st, err),
            "step 2 (B)");
     oza::GemmPlan plan{};
     plan.a_planes = aplanes;

@@ -363,10 +363,10 @@ bool oza_server::launch() {
         if (e == cudaSuccess) e = oza::launch_stats_cols(p.B, p.K, p.N, p.colmax, ex->sms, sl->st);
         if (e == cudaSuccess)
             e = oza::launch_slice_rows(scheme, p.A, p.M, p.K, p.shiftA, p.S, beta, p.k_param, p.a_planes, p.Mp, p.Kp,
-                                       ex->sms, sl->st);
+                                       ex->sms, sl->st, 0, err);
         if (e == cudaSuccess)
             e = oza::launch_slice_cols(scheme, p.B, p.K, p.N, p.colmax, p.k_param, p.S, beta, p.shiftB, p.b_planes,
-                                       p.Np, p.Kp, sl->st);
+                                       p.Np, p.Kp, sl->st, err);
         if (e == cudaSuccess) e = oza::launch_gemm_i8(g, sl->st);
         if (e == cudaSuccess && scheme == OZA_SCHEME2)
             e = oza::launch_crt_coef(p.coef, p.Mp, p.Np, p.M, p.N, p.S, p.shiftA, p.shiftB, p.C, ex->sms, sl->st);

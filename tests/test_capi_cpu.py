@@ -289,3 +289,19 @@ def test_reference_harnesses_build_against_drop_in_headers(src, tmp_path):
                     f"-L{root}/ozablas_b200", "-loza_b200", "-L/usr/local/cuda/lib64", "-lcublas"], check=True)
     syms = subprocess.run(["nm", "-u", "-C", str(exe)], capture_output=True, text=True, check=True).stdout
     assert "ozablas::CudaExecutor::CudaExecutor(int)" in syms
+
+
+def test_residue_slicer_knob():
+    """The process-wide slicer choice round-trips and rejects unknown modes
+    (no GPU call)."""
+    import ozablas_b200 as oz
+    saved = oz.residue_slicer()
+    try:
+        assert saved == oz.OZA_SLICER_TENSOR
+        oz.set_residue_slicer(oz.OZA_SLICER_CUDA_CORES)
+        assert oz.residue_slicer() == oz.OZA_SLICER_CUDA_CORES
+        with pytest.raises(ValueError):
+            oz.set_residue_slicer(7)
+        assert oz.residue_slicer() == oz.OZA_SLICER_CUDA_CORES
+    finally:
+        oz.set_residue_slicer(saved)
