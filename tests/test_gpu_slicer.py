@@ -128,3 +128,37 @@ def test_tensor_slicer_does_not_report_device_errors(executor, slicer_mode):
     for _ in range(5):
         oz.ozaki_scheme2_gemm(W, A, B, C)
     assert W.device_error() == 0
+
+
+def test_concurrent_calls_on_two_streams_are_bit_identical(slicer_mode):
+    """Calls issued on two streams at once put one call's tensor-core slicers
+    beside the other's GEMM or CRT on the same GPU, and the two calls' slicers
+    beside each other (TMEM shared by co-resident CTAs).  Every result must
+    equal the same call made alone, and no bounded wait may expire."""
+    import torch
+    oz = slicer_mode
+    oz.set_residue_slicer(oz.OZA_SLICER_TENSOR)
+    shapes = [(1024, 768, 2048, 16), (2048, 1024, 1024, 12)]
+    runs = []
+    for (M, N, K, S), seed in zip(shapes, (21, 31)):
+        ex = oz.CudaExecutor(0)
+        st = torch.cuda.Stream()
+        ex.set_stream(st)
+        A = torch.from_numpy(oz.generate_matrix(M, K, 1.0, seed)).cuda()
+        B = torch.from_numpy(oz.generate_matrix(K, N, 1.0, seed + 1)).cuda()
+        W = oz.WorkspaceScheme2(ex, M, N, K, S)
+        ref = torch.empty(M, N, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        oz.ozaki_scheme2_gemm(W, A, B, ref)
+        st.synchronize()
+        outs = [torch.full_like(ref, float("nan")) for _ in range(6)]
+        runs.append((ex, st, W, A, B, ref, outs))
+    torch.cuda.synchronize()
+    for k in range(6):           # interleaved issue: both streams busy at once
+        for ex, st, W, A, B, ref, outs in runs:
+            oz.ozaki_scheme2_gemm(W, A, B, outs[k])
+    torch.cuda.synchronize()
+    for ex, st, W, A, B, ref, outs in runs:
+        assert W.device_error() == 0
+        for C in outs:
+            assert torch.equal(C.view(torch.int64), ref.view(torch.int64))
