@@ -61,9 +61,10 @@ def parse():
                    help="offered loads as fractions of the batched server's measured capacity")
     p.add_argument("--materialize", action="store_true",
                    help="unfused path: INT32 products in HBM and a separate reconstruction kernel")
-    p.add_argument("--slicer", default="tensor", choices=["tensor", "cuda-cores"],
-                   help="Scheme II step-2 residue slicer for S <= 16: digit products on tcgen05 MMAs "
-                        "(default) or dp4a; identical planes")
+    p.add_argument("--slicer", default="auto", choices=["auto", "tensor", "cuda-cores"],
+                   help="Scheme II step-2 residue slicer: auto (default: tcgen05 digit products for "
+                        "12 <= S <= 16, dp4a below), tensor (tcgen05 for every S <= 16) or cuda-cores (dp4a); "
+                        "identical planes")
     p.add_argument("--overlap-chunks", type=int, default=0,
                    help="row chunks of the overlapped Scheme II stages (0: the library's rule; 1: the four "
                         "steps in order, one GEMM launch over all tiles)")
@@ -107,7 +108,7 @@ def workload(args):
                + ("larger than the 126 MB L2; no flush" if (M * K + K * N) * 8 > 126e6 else
                   "fit in L2: timings include L2 reuse")}
     # non-default settings are part of the workload's description
-    if getattr(args, "slicer", "tensor") != "tensor":
+    if getattr(args, "slicer", "auto") != "auto":
         w["slicer"] = args.slicer
     if getattr(args, "overlap_chunks", 0):
         w["overlap_chunks"] = args.overlap_chunks
@@ -373,7 +374,8 @@ def run_ours(args, ws, rank, local):
                                                                          materialize=args.materialize)
     if args.overlap_chunks:
         W.set_gemm_config(overlap_chunks=args.overlap_chunks)
-    oz.set_residue_slicer(oz.OZA_SLICER_TENSOR if args.slicer == "tensor" else oz.OZA_SLICER_CUDA_CORES)
+    oz.set_residue_slicer({"auto": oz.OZA_SLICER_AUTO, "tensor": oz.OZA_SLICER_TENSOR,
+                           "cuda-cores": oz.OZA_SLICER_CUDA_CORES}[args.slicer])
     gemm = oz.ozaki_scheme2_gemm if args.scheme == 2 else oz.ozaki_scheme1_gemm
     step = lambda: gemm(W, dA, dB, dC)   # noqa: E731
 

@@ -203,14 +203,19 @@ typedef struct {
 } oza_gemm_config_t;
 
 oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg); /* NULL: defaults */
-/* Process-wide choice of the Scheme II step-2 residue slicer for S <= 16:
- * OZA_SLICER_TENSOR (default) forms the digit products (sum_i d_i (256^i mod m))
- * with tcgen05 INT8 MMAs, OZA_SLICER_CUDA_CORES with dp4a.  The residue planes
- * are identical; the choice only changes speed.  Applies to calls issued
+/* Process-wide choice of the Scheme II step-2 residue slicer.  The tensor-core
+ * slicer forms the digit products (sum_i d_i (256^i mod m)) with tcgen05 INT8
+ * MMAs (S <= 16), the CUDA-core slicer with dp4a.  OZA_SLICER_AUTO (default)
+ * takes the tensor cores from S = 12 to 16, where they are as fast or faster,
+ * and dp4a below (at S <= 6 the MMA rounds' fixed cost outweighs the dp4a
+ * work they save); OZA_SLICER_TENSOR forces the tensor cores for every
+ * S <= 16; OZA_SLICER_CUDA_CORES forces dp4a.  The residue planes are
+ * identical; the choice only changes speed.  Applies to calls issued
  * afterwards.  Extension: the reference has one CUDA-core slicer
  * (src/pipeline/step2_slicing.hpp:110-206). */
-#define OZA_SLICER_TENSOR 0
+#define OZA_SLICER_AUTO 0
 #define OZA_SLICER_CUDA_CORES 1
+#define OZA_SLICER_TENSOR 2
 oza_status_t oza_set_residue_slicer(int mode);
 int oza_get_residue_slicer(void);
 oza_status_t oza_ws_get_gemm_config(oza_ws_t ws, oza_gemm_config_t* cfg);

@@ -28,7 +28,7 @@ __all__ = [
     "generate_matrix", "scheme1_beta", "scheme2_k_param", "lib", "exported_symbols", "block_error",
     "autotune_slices", "autotune_scheme", "GroupGemm", "Server", "slices_for_target", "scheme_for_target",
     "ozaki_gemm_host", "selftest_wait_timeout", "set_residue_slicer", "residue_slicer",
-    "OZA_SLICER_TENSOR", "OZA_SLICER_CUDA_CORES",
+    "OZA_SLICER_AUTO", "OZA_SLICER_TENSOR", "OZA_SLICER_CUDA_CORES",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -554,13 +554,14 @@ def ozaki_gemm_host(ws, A, B, C, timings: OzaTimings | None = None) -> None:
             setattr(timings, f, float(getattr(t, f)))
 
 
-OZA_SLICER_TENSOR, OZA_SLICER_CUDA_CORES = 0, 1
+OZA_SLICER_AUTO, OZA_SLICER_CUDA_CORES, OZA_SLICER_TENSOR = 0, 1, 2
 
 
 def set_residue_slicer(mode: int) -> None:
-    """Process-wide Scheme II step-2 slicer for S <= 16: OZA_SLICER_TENSOR
-    (default; digit products on tcgen05 INT8 MMAs) or OZA_SLICER_CUDA_CORES
-    (dp4a).  Both give identical residue planes."""
+    """Process-wide Scheme II step-2 slicer: OZA_SLICER_AUTO (default; tcgen05
+    digit products from S = 12 to 16, dp4a below), OZA_SLICER_TENSOR (tcgen05
+    for every S <= 16) or OZA_SLICER_CUDA_CORES (dp4a).  All give identical
+    residue planes."""
     _check(lib().oza_set_residue_slicer(int(mode)))
 
 

@@ -670,8 +670,9 @@ oza_status_t oza_ws_set_gemm_config(oza_ws_t ws, const oza_gemm_config_t* cfg) {
 }
 
 oza_status_t oza_set_residue_slicer(int mode) {
-    if (mode != OZA_SLICER_TENSOR && mode != OZA_SLICER_CUDA_CORES)
-        return fail(OZA_INVALID_ARG, "oza_set_residue_slicer: mode must be OZA_SLICER_TENSOR or OZA_SLICER_CUDA_CORES");
+    if (mode != OZA_SLICER_AUTO && mode != OZA_SLICER_TENSOR && mode != OZA_SLICER_CUDA_CORES)
+        return fail(OZA_INVALID_ARG,
+                    "oza_set_residue_slicer: mode must be OZA_SLICER_AUTO, OZA_SLICER_TENSOR or OZA_SLICER_CUDA_CORES");
     oza::set_residue_slicer(mode);
     return OZA_OK;
 }

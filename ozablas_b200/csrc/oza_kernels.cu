@@ -1972,7 +1972,16 @@ cudaError_t launch_stats_cols(const double* B, size_t rows, size_t cols, unsigne
     X(16) X(17) X(18) X(19) X(20)
 
 namespace {
-int g_residue_slicer = 0;   // 0: tensor-core digit products (S <= 16), 1: CUDA cores only
+int g_residue_slicer = 0;   // 0: tensor cores for kMmaSlicerMinS <= S <= 16, 1: CUDA cores only, 2: tensor cores for S <= 16
+// Smallest S at which the default takes the tensor-core slicers.  Step 2 at
+// 8192^3 / 4096^3 (ms, tensor / dp4a): S = 4 0.505 / 0.394, S = 8 0.712 /
+// 0.714, S = 12 0.880 / 0.890, S = 16 1.109 / 1.197; at S = 2 (4096^3)
+// 0.132 / 0.085.  Each MMA round has a fixed cost that a few moduli do not
+// amortise.
+constexpr int kMmaSlicerMinS = 12;
+bool use_mma_slicer(int S) {
+    return S <= 16 && (g_residue_slicer == 2 || (g_residue_slicer == 0 && S >= kMmaSlicerMinS));
+}
 
 template <int S>
 cudaError_t launch_rows_mma(const double* A, long long R, long long C, const int32_t* shift, int offset, int8_t* out,
@@ -2017,7 +2026,7 @@ cudaError_t launch_slice_rows(int scheme, const double* A, size_t rows, size_t c
     const int grid = grid_for(chunks, 256, sms);
     const long long R = (long long)rows, C = (long long)cols, RP = (long long)rows_p, CP = (long long)cols_p;
     const long long PR = plane_rows ? (long long)plane_rows : RP;
-    if (scheme == 2 && S <= 16 && k_param <= 62 && err && g_residue_slicer == 0) {
+    if (scheme == 2 && k_param <= 62 && err && use_mma_slicer(S)) {
         switch (S) {
 #define OZA_CASE(n) \
     case n: return launch_rows_mma<n>(A, R, C, shift, k_param, out, CP, PR, sms, err, st);
@@ -2052,7 +2061,7 @@ cudaError_t launch_slice_cols(int scheme, const double* B, size_t K, size_t N, c
     if (N > Np) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)((N + 31) / 32), (unsigned)(Kp / 128));
     const long long KK = (long long)K, NN = (long long)N, NP = (long long)Np, KP = (long long)Kp;
-    if (scheme == 2 && S <= 16 && offset <= 62 && err && g_residue_slicer == 0) {
+    if (scheme == 2 && offset <= 62 && err && use_mma_slicer(S)) {
         switch (S) {
 #define OZA_CASE(n) \
     case n: return launch_cols_mma<n>(B, KK, NN, colmax, offset, shift, out, NP, KP, err, st);

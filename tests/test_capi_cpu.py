@@ -297,7 +297,9 @@ def test_residue_slicer_knob():
     import ozablas_b200 as oz
     saved = oz.residue_slicer()
     try:
-        assert saved == oz.OZA_SLICER_TENSOR
+        assert saved == oz.OZA_SLICER_AUTO
+        oz.set_residue_slicer(oz.OZA_SLICER_TENSOR)
+        assert oz.residue_slicer() == oz.OZA_SLICER_TENSOR
         oz.set_residue_slicer(oz.OZA_SLICER_CUDA_CORES)
         assert oz.residue_slicer() == oz.OZA_SLICER_CUDA_CORES
         with pytest.raises(ValueError):
