@@ -41,8 +41,31 @@ __constant__ CrtTable c_crt[kMaxSlices];
 
 // The reference's moduli (src/common/crt_tables.hpp:13-16).  The residues are
 // only comparable with the same list in the same order.
-static const uint32_t kModuli[kMaxSlices] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
+constexpr uint32_t kModuli[kMaxSlices] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
                                              193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
+
+// 3 M < 2^(32 NL) for the product M of the first S moduli (NL = ceil(S/4)
+// 32-bit limbs of M): then T - q M (in [-M/2, 3M/2) for the quotient the CRT
+// finish picks), its comparison with floor(M/2) and its correction by M are
+// all signed values of NL limbs, so the finish can run on NL limbs, with T
+// and q M taken modulo 2^(32 NL).  True for every S except 4 and 8.
+__host__ __device__ constexpr bool crt_fits_nl(int S) {
+    uint32_t w[6] = {1, 0, 0, 0, 0, 0};
+    for (int i = 0; i <= S; ++i) {
+        const uint64_t f = i < S ? kModuli[i] : 3u;
+        uint64_t c = 0;
+        for (int l = 0; l < 6; ++l) {
+            const uint64_t v = (uint64_t)w[l] * f + c;
+            w[l] = (uint32_t)v;
+            c = v >> 32;
+        }
+    }
+    for (int l = (S + 3) / 4; l < 6; ++l)
+        if (w[l]) return false;
+    return true;
+}
+static_assert(crt_fits_nl(16) && crt_fits_nl(20) && crt_fits_nl(12) && !crt_fits_nl(8) && !crt_fits_nl(4),
+              "limb bound of the CRT finish");
 
 // ---------------------------------------------------------------------------
 // Host: constant tables
@@ -1020,6 +1043,11 @@ template <int N>
 __device__ __forceinline__ void mw_sub(uint32_t (&r)[N], const uint32_t (&x)[N], const uint32_t (&y)[N]);
 
 template <>
+__device__ __forceinline__ void mw_sub<1>(uint32_t (&r)[1], const uint32_t (&x)[1], const uint32_t (&y)[1]) {
+    r[0] = x[0] - y[0];
+}
+
+template <>
 __device__ __forceinline__ void mw_sub<2>(uint32_t (&r)[2], const uint32_t (&x)[2], const uint32_t (&y)[2]) {
     asm("sub.cc.u32 %0, %2, %4; subc.u32 %1, %3, %5;" : "=&r"(r[0]),"=&r"(r[1]) : "r"(x[0]),"r"(x[1]),"r"(y[0]),"r"(y[1]));
 }
@@ -1049,9 +1077,11 @@ __device__ __forceinline__ void mw_sub<6>(uint32_t (&r)[6], const uint32_t (&x)[
 // d0 + d1 2^64 + d2 2^128 over 64-bit limbs with a rounding after each
 // addition (crt_math.hpp:73-80), sign applied, scaled by 2^-esum
 // (step4_reconstruction.hpp:59-184).
-template <int NL>
+// FIT (crt_fits_nl(S)): the arithmetic runs on NL limbs, T and q M modulo
+// 2^(32 NL); otherwise on NL + 1.  The same bits either way.
+template <int NL, bool FIT = false>
 __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>& acc, int esum) {
-    constexpr int L = NL + 1;
+    constexpr int L = FIT ? NL : NL + 1;
     uint32_t t[L];
     unsigned long long carry = 0;
 #pragma unroll
@@ -1060,7 +1090,7 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
         t[l] = (uint32_t)v;
         carry = v >> 32;
     }
-    t[NL] = (uint32_t)carry;
+    if constexpr (L > NL) t[NL] = (uint32_t)carry;
     // nearest quotient: with the estimate within 2^-44 of T / M,
     // floor(estimate + 1/2 - 2^-40) is q* or q* - 1, so V = T - q M is either
     // the answer or the answer + M (then V >= floor(M/2)).
@@ -1083,13 +1113,13 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
     }
     mw_sub<L>(v, t, qm);
     mw_sub<L>(d, v, mh);
-    if ((int)d[NL] >= 0) {      // V >= floor(M/2): one M too many
+    if ((int)d[L - 1] >= 0) {      // V >= floor(M/2): one M too many
         uint32_t w[L];
         mw_sub<L>(w, v, m);
 #pragma unroll
         for (int l = 0; l < L; ++l) v[l] = w[l];
     }
-    const bool neg = (int)v[NL] < 0;
+    const bool neg = (int)v[L - 1] < 0;
     if (neg) {
         uint32_t z[L];
 #pragma unroll
@@ -1099,12 +1129,15 @@ __device__ __forceinline__ double crt_finish(const CrtTable& T, const CrtAcc<NL>
 #pragma unroll
         for (int l = 0; l < L; ++l) v[l] = w[l];
     }
-    double mag = __ull2double_rn((unsigned long long)v[0] | (NL > 1 ? (unsigned long long)v[1] << 32 : 0ull));
-    if (NL > 2) {
-        const unsigned long long w1 = (unsigned long long)v[2] | (NL > 3 ? (unsigned long long)v[3] << 32 : 0ull);
+    unsigned long long w0 = v[0];
+    if constexpr (NL > 1) w0 |= (unsigned long long)v[1] << 32;
+    double mag = __ull2double_rn(w0);
+    if constexpr (NL > 2) {
+        unsigned long long w1 = v[2];
+        if constexpr (NL > 3) w1 |= (unsigned long long)v[3] << 32;
         mag = __dadd_rn(mag, __ull2double_rn(w1) * 0x1p64);
     }
-    if (NL > 4) mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)v[4]) * 0x1p128);
+    if constexpr (NL > 4) mag = __dadd_rn(mag, __ull2double_rn((unsigned long long)v[4]) * 0x1p128);
     const int e = -esum;
     return scale_pow2(neg ? -mag : mag, e, pow2_or_zero(e));
 }
@@ -1560,7 +1593,7 @@ __device__ __forceinline__ void crt_coef_chunk(const uint8_t* __restrict__ coef,
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
         const long long j = j0 + e;
-        if (j < N) crow[j] = crt_finish<NL>(T, st[e], sa + sB[j]);
+        if (j < N) crow[j] = crt_finish<NL, crt_fits_nl(S)>(T, st[e], sa + sB[j]);
     }
 }
 

@@ -35,7 +35,7 @@ def _padding_zero(got):
     assert not got["B_planes"][:, :N, K:].any()
 
 
-@pytest.mark.parametrize("S", [1, 2, 4, 7, 8, 9, 12, 16, 18, 20])
+@pytest.mark.parametrize("S", [1, 2, 3, 4, 5, 7, 8, 9, 11, 12, 13, 15, 16, 17, 18, 20])
 def test_scheme2_stages_bitexact(executor, S):
     oz = _oz()
     from oracle import Oracle
